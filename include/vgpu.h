@@ -1,0 +1,273 @@
+/*
+ * vgpu.h -- C ABI of the B200 FDTD time-stepping engine.
+ *
+ * The engine replaces the time loop of the Vulture solver: the function
+ * propagate() (reference src/simulation.c:136-231, declared in
+ * src/simulation.h:41 and called from src/vulture.c:173) together with every
+ * update routine it calls.  Everything the reference sets up before that call
+ * (grid, media, PML/Mur/Debye/SIBC state, sources, plane waves, observers) is
+ * passed in as plain C data in a vgpu_problem.  No torch or CUDA type appears
+ * in this header.
+ *
+ * Conventions
+ *   - Face order XLO, XHI, YLO, YHI, ZLO, ZHI = 0..5 and field order
+ *     EX, EY, EZ, HX, HY, HZ = 0..5, as the reference's MeshFace and
+ *     FieldComponent enums (src/fdtd_types.h:86-110).
+ *   - A "limit" int32_t lim[6] is the inclusive index range
+ *     [lim[0]..lim[1]] x [lim[2]..lim[3]] x [lim[4]..lim[5]], as the
+ *     reference's field-limit arrays (src/grid.c:390-454).
+ *   - Volumes are n[0]*n[1]*n[2] values, index (i*n[1]+j)*n[2]+k with k
+ *     fastest: the reference's [i][j][k] arrays (src/alloc_array.c:54-141).
+ *     n[] counts the ghost cells (src/grid.c:380-383).
+ *   - All host inputs are double.  In VGPU_FP32 mode the engine rounds fields
+ *     and coefficients to float on upload; the DFT accumulators, Debye
+ *     recursion and waveform phase stay double.
+ *   - Every function returns 0 on success and a negative VGPU_E* code on
+ *     failure; vgpu_last_error() gives the message.  Nothing calls exit().
+ *   - The engine copies every input at vgpu_create(); the caller keeps
+ *     ownership of its arrays and may free them afterwards.
+ */
+#ifndef VGPU_H
+#define VGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VGPU_ABI_VERSION 1
+
+/* Status codes. */
+#define VGPU_OK            0
+#define VGPU_EINVAL       -1   /* invalid problem description or argument */
+#define VGPU_ENOMEM       -2   /* device or host allocation failed */
+#define VGPU_ECUDA        -3   /* CUDA runtime error */
+#define VGPU_ENODEV       -4   /* no usable sm_100 device */
+#define VGPU_ENONFINITE   -5   /* a field became NaN/Inf (finiteness check) */
+#define VGPU_ETIMEOUT     -6   /* a bounded device wait ran out */
+#define VGPU_ECANCELLED   -7   /* request cancelled (serving API) */
+
+typedef enum { VGPU_FP64 = 0, VGPU_FP32 = 1 } vgpu_precision;
+
+/* Treatment of the ghost layer on an external face (src/surface.c:569-812). */
+enum { VGPU_GHOST_NONE = 0, VGPU_GHOST_PEC = 1, VGPU_GHOST_PMC = 2, VGPU_GHOST_PERIODIC = 3 };
+
+/* Source kinds after the reference's init-time conversions (src/source.c:602-753). */
+enum {
+  VGPU_SRC_FIELD = 0,    /* F = soft*F + v                 (ST_EFIELD / ST_HFIELD) */
+  VGPU_SRC_CURRENT = 1   /* F = soft*F - coef(i,j,k)*v      (ST_ELEC/MAGN_CURR_DENSITY) */
+};
+
+/* Waveform types (src/waveform.h:44-57). */
+enum {
+  VGPU_WF_GAUSSIAN_PULSE = 0, VGPU_WF_NARROW_GAUSSIAN_PULSE, VGPU_WF_DIFF_GAUSSIAN_PULSE,
+  VGPU_WF_RICKER_WAVELET, VGPU_WF_MOD_GAUSSIAN_PULSE, VGPU_WF_COMPACT_PULSE,
+  VGPU_WF_DIFF_COMPACT_PULSE, VGPU_WF_MOD_COMPACT_PULSE, VGPU_WF_RAMPED_SINUSOID,
+  VGPU_WF_EXTERNAL
+};
+
+/* A waveform, evaluated on the device for the analytic plane-wave incident
+ * field (src/waveform.c:590-638).  table holds table_size rows of
+ * (t, value, second-derivative) for VGPU_WF_EXTERNAL (src/waveform.c:511-805). */
+typedef struct {
+  int32_t type;
+  int32_t table_size;
+  double size, delay, width, frequency;
+  const double *table;
+} vgpu_waveform;
+
+/* One source after init (src/source.c:469-599).  values[n] is the source
+ * amplitude size*wf(t) at the field's time of step n: n*dt for E components,
+ * (n+0.5)*dt for H components. */
+typedef struct {
+  int32_t field;       /* VGPU field index 0..5 */
+  int32_t kind;        /* VGPU_SRC_FIELD / VGPU_SRC_CURRENT */
+  int32_t soft;        /* 1 = soft (adds), 0 = hard (replaces) */
+  int32_t flim[6];
+  const double *values;
+} vgpu_source;
+
+/* A dispersive block of the Debye medium (src/debye.c:44-55).
+ * dalpha/dbeta hold num_poles complex values as (re, im) pairs. */
+typedef struct {
+  int32_t flim[3][6];  /* limits of Ex, Ey, Ez */
+  int32_t num_poles;
+  const double *dalpha;
+  const double *dbeta;
+} vgpu_debye;
+
+/* A total-field/scattered-field plane wave (src/planewave.c:47-93). */
+typedef struct {
+  int32_t active[6];          /* which Huygens faces correct fields */
+  int32_t flim[6][6][6];      /* [face][field][lim] correction limits */
+  int32_t waveform;           /* index into vgpu_problem.waveforms */
+  int32_t use_aux_grid;       /* 1: cubic grid, 1-D auxiliary grid (planewave.c:1226-1419) */
+  double delay;
+  double kinc[3];
+  double finc[6];
+  double r0[3];               /* origin, physical units */
+  double ijk0[3];             /* origin, grid indices */
+  double phase_velocity;
+  /* Auxiliary grid (use_aux_grid == 1). */
+  int32_t aux_nx, aux_xb, aux_npml;
+  double aux_beta, aux_gamma;
+  const double *aux_adx, *aux_bdx, *aux_ahx, *aux_bhx;   /* aux_npml each */
+  const double *aux_source;   /* num_steps: wf(n*dt) driving Eyi[0] */
+} vgpu_planewave;
+
+/* SIBC boundary model: 4x4 recursive-convolution filters (src/filter.h:40-73).
+ * For row p, column q: num_poles[p][q] poles starting at pole_offset[p][q] in
+ * q0/q1/q2 (complex, stored as re,im pairs), constant term asymp[p][q]. */
+typedef struct {
+  int32_t num_poles[4][4];
+  int32_t pole_offset[4][4];
+  double asymp[4][4];
+  const double *q0, *q1, *q2;
+} vgpu_sibc_model;
+
+/* An SIBC surface (src/sibc.c:43-58).  gbbox is extended by one in the
+ * normal direction as the reference does (src/sibc.c:236-251); its faces are
+ * the cells of gbbox, numbered (ii*nj + jj)*nk + kk.  A and B are the pre- and
+ * post-filter axis transforms for its orientation and angle. */
+typedef struct {
+  int32_t normal;
+  int32_t model;
+  int32_t gbbox[6];
+  double A[4][4], B[4][4];
+  const uint8_t *adjA;        /* [faces][4] */
+  const uint8_t *adjB;        /* [faces][4] */
+} vgpu_sibc_surface;
+
+/* One operation of the SIBC magnetic correction (src/sibc.c:616-776),
+ * applied to H component `comp` at volume index `index`, in list order:
+ *   kind 0: H = 0
+ *   kind 1: H = H + c * (d1 * E1)
+ *   kind 2: H = H + c * (n1 * (d1 * E1) + n2 * (d2 * E2))
+ * E1/E2 are tangential E values of face (surface s, face f, slot 0..3). */
+typedef struct {
+  int64_t index;
+  int32_t comp;
+  int32_t kind;
+  int32_t s1, f1, slot1;
+  int32_t s2, f2, slot2;
+  double c, d1, d2, n1, n2;
+} vgpu_sibc_hop;
+
+typedef struct {
+  int32_t abi_version;        /* VGPU_ABI_VERSION */
+  int32_t precision;          /* vgpu_precision */
+
+  /* Grid (src/grid.c:326-454, 583-679). */
+  int32_t n[3];
+  int32_t gibox[6];
+  int32_t gobox[6];
+  int32_t gfilim[6][6];       /* bulk update limits per field */
+  uint64_t num_steps;
+  double dt;
+  const double *ide[3];       /* inverse primary edge lengths, n[axis] each */
+  const double *idh[3];       /* inverse secondary edge lengths */
+  const double *coef[9];      /* alphaEx..z, betaEx..z, gammaHx..z volumes */
+
+  /* External faces. */
+  int32_t ghost[6];           /* VGPU_GHOST_* per face */
+
+  /* UPML (src/pml.c:44-84). */
+  int32_t pml_present[6];
+  int32_t pml_flim[6][6][6];  /* [region][field][lim] */
+  const double *pml_ad[3], *pml_bd[3], *pml_ah[3], *pml_bh[3], *pml_ibd[3], *pml_ibh[3];
+
+  /* First-order Mur (src/mur.c:46-52). */
+  int32_t mur_present[6];
+  int32_t mur_flim[6][6][6];
+  double mur_zeta[6];
+
+  /* Debye blocks. */
+  int32_t num_debye;
+  const vgpu_debye *debye;
+
+  /* SIBC surfaces. */
+  int32_t num_sibc_models;
+  const vgpu_sibc_model *sibc_models;
+  int32_t num_sibc;
+  const vgpu_sibc_surface *sibc;
+  int64_t num_sibc_hops;
+  const vgpu_sibc_hop *sibc_hops;
+
+  /* Sources, in mesh order. */
+  int32_t num_sources;
+  const vgpu_source *sources;
+
+  /* Plane waves, waveforms and the field-position tables used by the
+   * analytic incident field (src/grid.c:1429-1476): pos_node[a][i] is the
+   * mesh-line coordinate of grid index i on axis a, pos_half[a][i] the
+   * mid-edge coordinate. */
+  int32_t num_planewaves;
+  const vgpu_planewave *planewaves;
+  int32_t num_waveforms;
+  const vgpu_waveform *waveforms;
+  const double *pos_node[3];
+  const double *pos_half[3];
+
+  /* Point observers (src/observer.c:622-650).  All six components are
+   * sampled at the top of step n, before any update, when
+   * out_start <= n <= out_stop. */
+  uint64_t out_start, out_stop;
+  int32_t num_td;             /* time-domain points */
+  const int32_t *td_points;   /* [num_td][3] grid indices */
+  int32_t num_fd;             /* frequency-domain (running DFT) points */
+  const int32_t *fd_points;   /* [num_fd][3] */
+  int32_t num_freq;
+  const double *omega;        /* angular frequencies, num_freq */
+} vgpu_problem;
+
+typedef struct vgpu_engine vgpu_engine;
+
+/* Timing of the last vgpu_run, measured with CUDA events on the engine's
+ * stream. */
+typedef struct {
+  double run_ms;              /* device time of the last vgpu_run */
+  uint64_t steps;             /* steps in that run */
+  uint64_t kernel_launches;   /* engine kernels launched in that run */
+  uint64_t device_bytes;      /* device memory held by the engine */
+} vgpu_stats;
+
+/* Create an engine on the current CUDA device (cuda:0 unless the caller set
+ * another) and upload the problem.  Replaces the state the reference builds
+ * in src/vulture.c:95-148 before propagate(). */
+int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
+
+/* Advance nsteps time steps (the loop body of src/simulation.c:156-222),
+ * continuing from the engine's current step.  Returns once the device has
+ * finished. */
+int vgpu_run(vgpu_engine *engine, uint64_t nsteps);
+
+/* Copy time-domain samples to the host: out[(s*num_td + p)*6 + c] for the
+ * first `steps` steps of the output window. */
+int vgpu_read_td(vgpu_engine *engine, double *out, uint64_t steps);
+
+/* Copy the running DFTs: re/im[(p*6 + c)*num_freq + f] (src/observer.c:857-899). */
+int vgpu_read_dft(vgpu_engine *engine, double *re, double *im);
+
+/* Copy one field component volume (0..5) to the host in the volume layout. */
+int vgpu_read_field(vgpu_engine *engine, int32_t component, double *out);
+
+/* Overwrite one field component volume (used to plant host-prepared state). */
+int vgpu_write_field(vgpu_engine *engine, int32_t component, const double *in);
+
+/* Scan all fields for NaN/Inf on the device; returns VGPU_ENONFINITE if any. */
+int vgpu_check_finite(vgpu_engine *engine);
+
+uint64_t vgpu_current_step(const vgpu_engine *engine);
+int vgpu_get_stats(const vgpu_engine *engine, vgpu_stats *stats);
+void vgpu_destroy(vgpu_engine *engine);
+
+/* Message of the last error on this thread. */
+const char *vgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VGPU_H */

@@ -1,0 +1,913 @@
+// engine.cu -- the vgpu C ABI (include/vgpu.h) on one B200.
+//
+// vgpu_create uploads a vgpu_problem into device memory (fields and
+// coefficients as padded [n0][n1][n2p] volumes, k rows aligned to 32
+// elements), builds the launch plan of one time step in the reference's order
+// (src/simulation.c:156-222), and captures a chunk of steps in a CUDA graph.
+// vgpu_run replays the graph; the running DFT of the frequency-domain
+// observers is accumulated every chunk from a buffer of field samples.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "kernels.cuh"
+
+using namespace vgpu_dev;
+
+static thread_local char g_err[1024];
+
+static int set_err(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+extern "C" const char *vgpu_last_error(void) { return g_err; }
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return set_err(VGPU_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+static const int kChunk = 64;      // steps per captured graph and per DFT block
+static const int kTB = kChunk;     // DFT staging rows
+
+__global__ void k_advance(uint64_t *step) { *step += 1; }
+
+struct DevAlloc {
+  std::vector<void *> ptrs;
+  uint64_t bytes = 0;
+  template <typename U>
+  int alloc(U **p, size_t count)
+  {
+    size_t b = sizeof(U) * (count ? count : 1);
+    cudaError_t e = cudaMalloc((void **)p, b);
+    if (e != cudaSuccess) return set_err(VGPU_ENOMEM, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
+    ptrs.push_back(*p);
+    bytes += b;
+    return 0;
+  }
+  void free_all()
+  {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual int run(uint64_t n) = 0;
+  virtual int read_td(double *out, uint64_t steps) = 0;
+  virtual int read_dft(double *re, double *im) = 0;
+  virtual int read_field(int c, double *out) = 0;
+  virtual int write_field(int c, const double *in) = 0;
+  virtual int check_finite() = 0;
+  uint64_t step = 0;
+  vgpu_stats stats{};
+};
+
+struct SrcLaunch {
+  Box b;
+  int c, kind;
+  double soft;
+  void *values;
+};
+
+template <typename T>
+struct PwLaunch {
+  PwView<T> pv;
+  TfsfView te, th;
+  int64_t total_e = 0, total_h = 0;
+};
+
+template <typename T>
+struct Engine : EngineBase {
+  vgpu_problem p{};
+  cudaStream_t s = nullptr;
+  DevAlloc mem;
+  Grid<T> g{};
+  int n2p = 0;
+  int64_t vol = 0;
+  T *fields = nullptr;
+  uint64_t *d_step = nullptr;
+  // bulk
+  Box be[3], bh[3], ube, ubh;
+  // PML
+  bool has_pml = false;
+  PmlView<T> pv{};
+  dim3 pml_grid;
+  // Mur
+  MurView mve{}, mvh{};
+  int64_t mur_total_e = 0, mur_total_h = 0;
+  // Debye
+  DebyeItem *d_debye = nullptr;
+  int n_debye = 0;
+  int64_t debye_total = 0;
+  double2 *d_J = nullptr, *d_dcoef = nullptr;
+  T *d_lastE = nullptr;
+  // SIBC
+  int nsibc = 0;
+  SibcSurf *d_surfs = nullptr;
+  SibcModelDev *d_models = nullptr;
+  double2 *d_q0 = nullptr, *d_q1 = nullptr, *d_q2 = nullptr, *d_zeta = nullptr;
+  double *d_old = nullptr;
+  uint8_t *d_adjA = nullptr, *d_adjB = nullptr;
+  int64_t *d_zofs = nullptr;
+  T *d_etan = nullptr;
+  int64_t sibc_faces = 0;
+  int64_t *d_tgt_index = nullptr, *d_tgt_start = nullptr;
+  int *d_tgt_comp = nullptr;
+  SibcOp *d_ops = nullptr;
+  int64_t ntgt = 0;
+  // sources and plane waves
+  std::vector<SrcLaunch> srcs;
+  std::vector<PwLaunch<T>> pws;
+  // ghost
+  GhostView gv{};
+  bool ghost_e = false, ghost_h = false;
+  int ghost_threads = 0;
+  // observers
+  int *d_td_pts = nullptr, *d_fd_pts = nullptr;
+  T *d_td = nullptr;
+  double *d_stage = nullptr, *d_re = nullptr, *d_im = nullptr, *d_omega = nullptr;
+  double2 *d_tw = nullptr;
+  uint64_t nout = 0;
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  uint64_t launches_per_step = 0;
+
+  ~Engine() override
+  {
+    if (graph) cudaGraphExecDestroy(graph);
+    mem.free_all();
+    if (s) cudaStreamDestroy(s);
+  }
+
+  template <typename U>
+  int upload(U **d, const U *h, size_t n)
+  {
+    if (mem.alloc(d, n)) return VGPU_ENOMEM;
+    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, s));
+    return 0;
+  }
+
+  int upload_real(T **d, const double *h, size_t n)
+  {
+    std::vector<T> tmp(n ? n : 1);
+    for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
+    if (mem.alloc(d, n)) return VGPU_ENOMEM;
+    if (n) CK(cudaMemcpy(*d, tmp.data(), sizeof(T) * n, cudaMemcpyHostToDevice));
+    return 0;
+  }
+
+  // Host volume [n0][n1][n2] -> padded device volume.
+  int upload_volume(T *d, const double *h)
+  {
+    std::vector<T> tmp((size_t)vol, (T)0);
+    for (int i = 0; i < p.n[0]; i++)
+      for (int j = 0; j < p.n[1]; j++) {
+        const double *src = h + ((int64_t)i * p.n[1] + j) * p.n[2];
+        T *dst = tmp.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
+        for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
+      }
+    CK(cudaMemcpy(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice));
+    return 0;
+  }
+
+  int create(const vgpu_problem *in)
+  {
+    p = *in;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    n2p = (p.n[2] + 31) / 32 * 32;
+    g.n0 = p.n[0];
+    g.n1 = p.n[1];
+    g.n2 = p.n[2];
+    g.s1 = n2p;
+    g.s0 = (int64_t)p.n[1] * n2p;
+    vol = (int64_t)p.n[0] * g.s0;
+    if (mem.alloc(&fields, (size_t)vol * 6)) return VGPU_ENOMEM;
+    CK(cudaMemset(fields, 0, sizeof(T) * vol * 6));
+    for (int c = 0; c < 6; c++) g.F[c] = fields + (int64_t)c * vol;
+    T *coef = nullptr;
+    if (mem.alloc(&coef, (size_t)vol * 9)) return VGPU_ENOMEM;
+    for (int q = 0; q < 9; q++) {
+      if (int rc = upload_volume(coef + (int64_t)q * vol, p.coef[q])) return rc;
+      g.cf[q] = coef + (int64_t)q * vol;
+    }
+    for (int a = 0; a < 3; a++) {
+      T *d;
+      if (int rc = upload_real(&d, p.ide[a], p.n[a])) return rc;
+      g.ide[a] = d;
+      if (int rc = upload_real(&d, p.idh[a], p.n[a])) return rc;
+      g.idh[a] = d;
+    }
+    if (mem.alloc(&d_step, 1)) return VGPU_ENOMEM;
+    CK(cudaMemset(d_step, 0, sizeof(uint64_t)));
+
+    // Bulk limits.
+    for (int c = 0; c < 3; c++) {
+      be[c] = box_from(p.gfilim[c]);
+      bh[c] = box_from(p.gfilim[3 + c]);
+    }
+    ube = unite(be);
+    ubh = unite(bh);
+
+    if (int rc = setup_pml()) return rc;
+    setup_mur();
+    if (int rc = setup_debye()) return rc;
+    if (int rc = setup_sibc()) return rc;
+    if (int rc = setup_sources()) return rc;
+    if (int rc = setup_planewaves()) return rc;
+    setup_ghost();
+    if (int rc = setup_observers()) return rc;
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    stats.device_bytes = mem.bytes;
+    return capture_graph();
+  }
+
+  static Box unite(const Box b[3])
+  {
+    Box u{ 1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30) };
+    for (int c = 0; c < 3; c++) {
+      if (b[c].empty()) continue;
+      u.i0 = std::min(u.i0, b[c].i0); u.i1 = std::max(u.i1, b[c].i1);
+      u.j0 = std::min(u.j0, b[c].j0); u.j1 = std::max(u.j1, b[c].j1);
+      u.k0 = std::min(u.k0, b[c].k0); u.k1 = std::max(u.k1, b[c].k1);
+    }
+    return u;
+  }
+
+  int setup_pml()
+  {
+    pv.nreg = 0;
+    int plane = 0, maxj = 1, maxk = 1;
+    for (int r = 0; r < 6; r++) {
+      if (!p.pml_present[r]) continue;
+      int q = pv.nreg++;
+      Box bb[6];
+      for (int f = 0; f < 6; f++) bb[f] = box_from(p.pml_flim[r][f]);
+      for (int f = 0; f < 6; f++) pv.lim[q][f] = bb[f];
+      Box all[6] = { bb[0], bb[1], bb[2], bb[3], bb[4], bb[5] };
+      Box ue = unite(all), uh = unite(all + 3);
+      Box u{ std::min(ue.i0, uh.i0), std::max(ue.i1, uh.i1), std::min(ue.j0, uh.j0), std::max(ue.j1, uh.j1),
+             std::min(ue.k0, uh.k0), std::max(ue.k1, uh.k1) };
+      pv.uni[q] = u;
+      pv.reg_plane0[q] = plane;
+      plane += u.ni();
+      maxj = std::max(maxj, u.nj());
+      maxk = std::max(maxk, u.nk());
+      for (int c = 0; c < 3; c++) {
+        int64_t ne = bb[c].count(), nh = bb[3 + c].count();
+        if (mem.alloc(&pv.PP[q][c], ne) || mem.alloc(&pv.P[q][c], ne) || mem.alloc(&pv.B[q][c], nh)) return VGPU_ENOMEM;
+        CK(cudaMemset(pv.PP[q][c], 0, sizeof(T) * (ne ? ne : 1)));
+        CK(cudaMemset(pv.P[q][c], 0, sizeof(T) * (ne ? ne : 1)));
+        CK(cudaMemset(pv.B[q][c], 0, sizeof(T) * (nh ? nh : 1)));
+      }
+    }
+    pv.reg_plane0[pv.nreg] = plane;
+    has_pml = pv.nreg > 0;
+    if (!has_pml) return 0;
+    for (int a = 0; a < 3; a++) {
+      T *d;
+      if (int rc = upload_real(&d, p.pml_ad[a], p.n[a])) return rc; pv.ad[a] = d;
+      if (int rc = upload_real(&d, p.pml_bd[a], p.n[a])) return rc; pv.bd[a] = d;
+      if (int rc = upload_real(&d, p.pml_ah[a], p.n[a])) return rc; pv.ah[a] = d;
+      if (int rc = upload_real(&d, p.pml_bh[a], p.n[a])) return rc; pv.bh[a] = d;
+      if (int rc = upload_real(&d, p.pml_ibd[a], p.n[a])) return rc; pv.ibd[a] = d;
+      if (int rc = upload_real(&d, p.pml_ibh[a], p.n[a])) return rc; pv.ibh[a] = d;
+    }
+    pml_grid = dim3((maxk + 31) / 32, (maxj + 7) / 8, plane);
+    return 0;
+  }
+
+  void setup_mur()
+  {
+    mve.nitems = mvh.nitems = 0;
+    mur_total_e = mur_total_h = 0;
+    for (int f = 0; f < 6; f++) {
+      mve.zeta[f] = mvh.zeta[f] = p.mur_zeta[f];
+      if (!p.mur_present[f]) continue;
+      int a = f / 2;
+      int dir = (f % 2 == 0) ? +1 : -1;
+      int comps[2];
+      if (a == 0) { comps[0] = EY; comps[1] = EZ; }
+      else if (a == 1) { comps[0] = EX; comps[1] = EZ; }
+      else { comps[0] = EY; comps[1] = EX; }
+      for (int cc = 0; cc < 2; cc++) {
+        Box b = box_from(p.mur_flim[f][comps[cc]]);
+        if (b.empty()) continue;
+        MurItem &m = mve.it[mve.nitems++];
+        m.b = b; m.c = comps[cc]; m.axis = a; m.dir = dir; m.face = f; m.first = mur_total_e;
+        mur_total_e += b.count();
+      }
+      Box b = box_from(p.mur_flim[f][HX + a]);
+      if (!b.empty()) {
+        MurItem &m = mvh.it[mvh.nitems++];
+        m.b = b; m.c = HX + a; m.axis = a; m.dir = 0; m.face = f; m.first = mur_total_h;
+        mur_total_h += b.count();
+      }
+    }
+  }
+
+  int setup_debye()
+  {
+    std::vector<DebyeItem> items;
+    std::vector<double2> coefs;
+    int64_t total = 0, jtot = 0, etot = 0;
+    for (int b = 0; b < p.num_debye; b++) {
+      const vgpu_debye &d = p.debye[b];
+      int ofs = (int)coefs.size();
+      for (int q = 0; q < d.num_poles; q++) coefs.push_back(make_double2(d.dalpha[2 * q], d.dalpha[2 * q + 1]));
+      for (int q = 0; q < d.num_poles; q++) coefs.push_back(make_double2(d.dbeta[2 * q], d.dbeta[2 * q + 1]));
+      for (int c = 0; c < 3; c++) {
+        Box bx = box_from(d.flim[c]);
+        if (bx.empty()) continue;
+        DebyeItem it{};
+        it.b = bx; it.c = c; it.np = d.num_poles; it.first = total; it.jofs = jtot; it.eofs = etot; it.coef_ofs = ofs;
+        items.push_back(it);
+        total += bx.count();
+        jtot += bx.count() * d.num_poles;
+        etot += bx.count();
+      }
+    }
+    n_debye = (int)items.size();
+    debye_total = total;
+    if (!n_debye) return 0;
+    if (int rc = upload(&d_debye, items.data(), items.size())) return rc;
+    if (int rc = upload(&d_dcoef, coefs.data(), coefs.size())) return rc;
+    if (mem.alloc(&d_J, jtot) || mem.alloc(&d_lastE, etot)) return VGPU_ENOMEM;
+    CK(cudaMemset(d_J, 0, sizeof(double2) * (jtot ? jtot : 1)));
+    CK(cudaMemset(d_lastE, 0, sizeof(T) * (etot ? etot : 1)));
+    return 0;
+  }
+
+  int setup_sibc()
+  {
+    nsibc = p.num_sibc;
+    if (!nsibc) return 0;
+    std::vector<SibcModelDev> models(p.num_sibc_models);
+    int total_poles = 0;
+    for (int m = 0; m < p.num_sibc_models; m++) {
+      const vgpu_sibc_model &sm = p.sibc_models[m];
+      models[m].poles = 0;
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) {
+          models[m].np[a][b] = sm.num_poles[a][b];
+          models[m].off[a][b] = sm.pole_offset[a][b];
+          models[m].asymp[a][b] = sm.asymp[a][b];
+          models[m].poles += sm.num_poles[a][b];
+          total_poles = std::max(total_poles, sm.pole_offset[a][b] + sm.num_poles[a][b]);
+        }
+    }
+    std::vector<double2> q0(total_poles + 1), q1(total_poles + 1), q2(total_poles + 1);
+    if (p.num_sibc_models) {
+      const vgpu_sibc_model &sm = p.sibc_models[0];
+      for (int r = 0; r < total_poles; r++) {
+        q0[r] = make_double2(sm.q0[2 * r], sm.q0[2 * r + 1]);
+        q1[r] = make_double2(sm.q1[2 * r], sm.q1[2 * r + 1]);
+        q2[r] = make_double2(sm.q2[2 * r], sm.q2[2 * r + 1]);
+      }
+    }
+    std::vector<SibcSurf> surfs(nsibc);
+    std::vector<int64_t> zofs(nsibc + 1), base(nsibc + 1);
+    std::vector<uint8_t> adjA, adjB;
+    int64_t faces = 0, z = 0;
+    for (int q = 0; q < nsibc; q++) {
+      const vgpu_sibc_surface &sf = p.sibc[q];
+      SibcSurf &o = surfs[q];
+      o.g = Box{ sf.gbbox[0], sf.gbbox[1] - 1, sf.gbbox[2], sf.gbbox[3] - 1, sf.gbbox[4], sf.gbbox[5] - 1 };
+      o.normal = sf.normal;
+      o.model = sf.model;
+      o.first = faces;
+      memcpy(o.A, sf.A, sizeof o.A);
+      memcpy(o.B, sf.B, sizeof o.B);
+      int64_t nf = o.g.count();
+      base[q] = faces;
+      zofs[q] = z;
+      adjA.insert(adjA.end(), sf.adjA, sf.adjA + 4 * nf);
+      adjB.insert(adjB.end(), sf.adjB, sf.adjB + 4 * nf);
+      faces += nf;
+      z += nf * models[sf.model].poles;
+    }
+    sibc_faces = faces;
+    if (upload(&d_surfs, surfs.data(), surfs.size()) || upload(&d_models, models.data(), models.size()) ||
+        upload(&d_q0, q0.data(), q0.size()) || upload(&d_q1, q1.data(), q1.size()) ||
+        upload(&d_q2, q2.data(), q2.size()) || upload(&d_adjA, adjA.data(), adjA.size()) ||
+        upload(&d_adjB, adjB.data(), adjB.size()) || upload(&d_zofs, zofs.data(), zofs.size()))
+      return VGPU_ENOMEM;
+    if (mem.alloc(&d_zeta, z) || mem.alloc(&d_old, faces * 16) || mem.alloc(&d_etan, faces * 4)) return VGPU_ENOMEM;
+    CK(cudaMemset(d_zeta, 0, sizeof(double2) * (z ? z : 1)));
+    CK(cudaMemset(d_old, 0, sizeof(double) * (faces ? faces * 16 : 1)));
+    CK(cudaMemset(d_etan, 0, sizeof(T) * (faces ? faces * 4 : 1)));
+    // Magnetic correction targets (ops arrive sorted by target).
+    std::vector<int64_t> tidx, tstart;
+    std::vector<int> tcomp;
+    std::vector<SibcOp> ops((size_t)p.num_sibc_hops + 1);
+    for (int64_t h = 0; h < p.num_sibc_hops; h++) {
+      const vgpu_sibc_hop &o = p.sibc_hops[h];
+      int i = (int)(o.index / ((int64_t)p.n[1] * p.n[2]));
+      int j = (int)((o.index / p.n[2]) % p.n[1]);
+      int k = (int)(o.index % p.n[2]);
+      int64_t dx = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
+      if (h == 0 || o.index != p.sibc_hops[h - 1].index || o.comp != p.sibc_hops[h - 1].comp) {
+        tidx.push_back(dx);
+        tcomp.push_back(o.comp);
+        tstart.push_back(h);
+      }
+      SibcOp &d = ops[h];
+      d.kind = o.kind;
+      d.c = o.c; d.d1 = o.d1; d.d2 = o.d2; d.n1 = o.n1; d.n2 = o.n2;
+      d.e1 = 4 * (base[o.s1] + o.f1) + o.slot1;
+      d.e2 = 4 * (base[o.s2] + o.f2) + o.slot2;
+    }
+    tstart.push_back(p.num_sibc_hops);
+    ntgt = (int64_t)tidx.size();
+    if (upload(&d_tgt_index, tidx.data(), tidx.size()) || upload(&d_tgt_comp, tcomp.data(), tcomp.size()) ||
+        upload(&d_tgt_start, tstart.data(), tstart.size()) || upload(&d_ops, ops.data(), ops.size()))
+      return VGPU_ENOMEM;
+    return 0;
+  }
+
+  int setup_sources()
+  {
+    for (int q = 0; q < p.num_sources; q++) {
+      const vgpu_source &src = p.sources[q];
+      SrcLaunch l{};
+      l.b = box_from(src.flim);
+      l.c = src.field;
+      l.kind = src.kind;
+      l.soft = src.soft;
+      T *d;
+      if (int rc = upload_real(&d, src.values, p.num_steps)) return rc;
+      l.values = d;
+      if (!l.b.empty()) srcs.push_back(l);
+    }
+    return 0;
+  }
+
+  int setup_planewaves()
+  {
+    static const int face_order[6] = { 2, 3, 4, 5, 0, 1 };  // YLO YHI ZLO ZHI XLO XHI
+    // (component, incident component, sign) per face for E and for H (src/planewave.c:576-1007).
+    static const int ecorr[6][2][3] = {
+      { { EY, HZ, +1 }, { EZ, HY, -1 } },  // XLO
+      { { EY, HZ, -1 }, { EZ, HY, +1 } },  // XHI
+      { { EX, HZ, -1 }, { EZ, HX, +1 } },  // YLO
+      { { EX, HZ, +1 }, { EZ, HX, -1 } },  // YHI
+      { { EX, HY, +1 }, { EY, HX, -1 } },  // ZLO
+      { { EX, HY, -1 }, { EY, HX, +1 } },  // ZHI
+    };
+    static const int hcorr[6][2][3] = {
+      { { HZ, EY, +1 }, { HY, EZ, -1 } },  // XLO
+      { { HZ, EY, -1 }, { HY, EZ, +1 } },  // XHI
+      { { HZ, EX, -1 }, { HX, EZ, +1 } },  // YLO
+      { { HZ, EX, +1 }, { HX, EZ, -1 } },  // YHI
+      { { HY, EX, +1 }, { HX, EY, -1 } },  // ZLO
+      { { HY, EX, -1 }, { HX, EY, +1 } },  // ZHI
+    };
+    std::vector<const double *> pos;
+    double *pn[3], *ph[3];
+    if (p.num_planewaves) {
+      for (int a = 0; a < 3; a++) {
+        if (upload(&pn[a], p.pos_node[a], p.n[a]) || upload(&ph[a], p.pos_half[a], p.n[a])) return VGPU_ENOMEM;
+      }
+    }
+    for (int q = 0; q < p.num_planewaves; q++) {
+      const vgpu_planewave &w = p.planewaves[q];
+      PwLaunch<T> L{};
+      PwView<T> &v = L.pv;
+      v.use_aux = w.use_aux_grid;
+      const vgpu_waveform &wf = p.waveforms[w.waveform];
+      v.wf.type = wf.type; v.wf.table_size = wf.table_size; v.wf.size = wf.size; v.wf.delay = wf.delay;
+      v.wf.width = wf.width; v.wf.frequency = wf.frequency; v.wf.table = nullptr;
+      if (wf.type == VGPU_WF_EXTERNAL) {
+        double *dt_;
+        if (upload(&dt_, wf.table, (size_t)wf.table_size * 3)) return VGPU_ENOMEM;
+        v.wf.table = dt_;
+      }
+      v.delay = w.delay;
+      v.phase_velocity = w.phase_velocity;
+      for (int a = 0; a < 3; a++) {
+        v.kinc[a] = w.kinc[a]; v.r0[a] = w.r0[a]; v.ijk0[a] = w.ijk0[a];
+        v.pos_node[a] = pn[a]; v.pos_half[a] = ph[a];
+      }
+      for (int c = 0; c < 6; c++) v.finc[c] = w.finc[c];
+      if (w.use_aux_grid) {
+        v.nx = w.aux_nx;
+        v.xb = w.aux_xb;
+        v.beta = (T)w.aux_beta;
+        v.gamma = (T)w.aux_gamma;
+        double mu0 = 4.0 * (4.0 * atan(1.0)) * 1e-7;
+        v.eta0 = (T)sqrt(mu0 / (1.0 / (mu0 * 299792458.0 * 299792458.0)));
+        if (mem.alloc(&v.Eyi, w.aux_nx + 2) || mem.alloc(&v.Hzi, w.aux_nx + 2) || mem.alloc(&v.PPyi, w.aux_npml) ||
+            mem.alloc(&v.Pyi, w.aux_npml) || mem.alloc(&v.Bzi, w.aux_npml))
+          return VGPU_ENOMEM;
+        CK(cudaMemset(v.Eyi, 0, sizeof(T) * (w.aux_nx + 2)));
+        CK(cudaMemset(v.Hzi, 0, sizeof(T) * (w.aux_nx + 2)));
+        CK(cudaMemset(v.PPyi, 0, sizeof(T) * w.aux_npml));
+        CK(cudaMemset(v.Pyi, 0, sizeof(T) * w.aux_npml));
+        CK(cudaMemset(v.Bzi, 0, sizeof(T) * w.aux_npml));
+        T *d;
+        if (upload_real(&d, w.aux_adx, w.aux_npml)) return VGPU_ENOMEM; v.adx = d;
+        if (upload_real(&d, w.aux_bdx, w.aux_npml)) return VGPU_ENOMEM; v.bdx = d;
+        if (upload_real(&d, w.aux_ahx, w.aux_npml)) return VGPU_ENOMEM; v.ahx = d;
+        if (upload_real(&d, w.aux_bhx, w.aux_npml)) return VGPU_ENOMEM; v.bhx = d;
+        if (upload_real(&d, w.aux_source, p.num_steps)) return VGPU_ENOMEM; v.source = d;
+      }
+      L.te.n = L.th.n = 0;
+      for (int o = 0; o < 6; o++) {
+        int f = face_order[o];
+        if (!w.active[f]) continue;
+        int a = f / 2;
+        bool lo = f % 2 == 0;
+        for (int e = 0; e < 2; e++) {
+          Box b = box_from(w.flim[f][ecorr[f][e][0]]);
+          if (!b.empty()) {
+            TfsfItem &it = L.te.it[L.te.n++];
+            it.b = b; it.c = ecorr[f][e][0]; it.inc = ecorr[f][e][1]; it.sign = ecorr[f][e][2];
+            it.axis = a; it.shift = lo ? -1 : 0; it.first = L.total_e;
+            L.total_e += b.count();
+          }
+          b = box_from(w.flim[f][hcorr[f][e][0]]);
+          if (!b.empty()) {
+            TfsfItem &it = L.th.it[L.th.n++];
+            it.b = b; it.c = hcorr[f][e][0]; it.inc = hcorr[f][e][1]; it.sign = hcorr[f][e][2];
+            it.axis = a; it.shift = lo ? +1 : 0; it.first = L.total_h;
+            L.total_h += b.count();
+          }
+        }
+      }
+      pws.push_back(L);
+    }
+    return 0;
+  }
+
+  void setup_ghost()
+  {
+    int maxp = 1;
+    for (int f = 0; f < 6; f++) {
+      gv.mode[f] = p.ghost[f];
+      if (p.ghost[f] != VGPU_GHOST_NONE) ghost_e = ghost_h = true;
+    }
+    for (int a = 0; a < 3; a++) {
+      gv.go_lo[a] = p.gobox[2 * a];
+      gv.go_hi[a] = p.gobox[2 * a + 1];
+    }
+    for (int a = 0; a < 3; a++) {
+      int b = (a + 1) % 3, c = (a + 2) % 3;
+      int np = (gv.go_hi[b] - gv.go_lo[b] + 2) * (gv.go_hi[c] - gv.go_lo[c] + 2);
+      maxp = std::max(maxp, np);
+    }
+    ghost_threads = maxp;
+  }
+
+  int setup_observers()
+  {
+    if (p.num_steps > 0 && p.out_start < p.num_steps)
+      nout = (p.out_stop < p.num_steps - 1 ? p.out_stop : p.num_steps - 1) - p.out_start + 1;
+    if (upload(&d_td_pts, p.td_points, (size_t)p.num_td * 3) || upload(&d_fd_pts, p.fd_points, (size_t)p.num_fd * 3))
+      return VGPU_ENOMEM;
+    if (mem.alloc(&d_td, (size_t)nout * p.num_td * 6)) return VGPU_ENOMEM;
+    size_t npc = (size_t)p.num_fd * 6;
+    if (mem.alloc(&d_stage, npc * kTB) || mem.alloc(&d_re, npc * p.num_freq) || mem.alloc(&d_im, npc * p.num_freq) ||
+        mem.alloc(&d_tw, (size_t)kTB * p.num_freq))
+      return VGPU_ENOMEM;
+    CK(cudaMemset(d_re, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
+    CK(cudaMemset(d_im, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
+    if (upload(&d_omega, p.omega, p.num_freq)) return VGPU_ENOMEM;
+    return 0;
+  }
+
+  static unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
+
+  // One time step, in the order of src/simulation.c:156-222.
+  int enqueue_step()
+  {
+    uint64_t launches = 0;
+    const dim3 blk(32, 8);
+    if (p.num_td || p.num_fd) {
+      int nt = (p.num_td + p.num_fd) * 6;
+      k_observe<T><<<blocks_for(nt, 128), 128, 0, s>>>(g, d_td_pts, p.num_td, d_fd_pts, p.num_fd, d_td, d_stage, d_step,
+                                                        0, p.out_start, p.out_stop, kTB);
+      launches++;
+    }
+    if (has_pml) { k_pml_e<T><<<pml_grid, blk, 0, s>>>(g, pv); launches++; }
+    if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
+    if (!ube.empty()) {
+      dim3 grd((ube.nk() + 31) / 32, (ube.nj() + 7) / 8, ube.ni());
+      k_bulk_e<T><<<grd, blk, 0, s>>>(g, be[0], be[1], be[2], ube);
+      launches++;
+    }
+    if (n_debye) {
+      k_debye<T><<<blocks_for(debye_total, 128), 128, 0, s>>>(g, d_debye, n_debye, debye_total, d_J, d_lastE, d_dcoef);
+      launches++;
+    }
+    if (nsibc) {
+      k_sibc_e<T><<<blocks_for(sibc_faces, 128), 128, 0, s>>>(g, d_surfs, nsibc, d_models, d_q0, d_q1, d_q2, d_adjA,
+                                                              d_adjB, d_zofs, d_zeta, d_old, d_etan, sibc_faces);
+      launches++;
+    }
+    for (auto &l : srcs)
+      if (l.c <= EZ) {
+        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, 0);
+        launches++;
+      }
+    for (auto &w : pws) {
+      if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, 0); launches++; }
+      if (w.total_e) {
+        k_tfsf<T><<<blocks_for(w.total_e, 128), 128, 0, s>>>(g, w.pv, w.te, w.total_e, p.dt, d_step, 0, 1);
+        launches++;
+      }
+    }
+    if (ghost_e) {
+      k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 6), 128, 0, s>>>(g, gv, 1, 0);
+      launches++;
+    }
+    if (has_pml) { k_pml_h<T><<<pml_grid, blk, 0, s>>>(g, pv); launches++; }
+    if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
+    if (!ubh.empty()) {
+      dim3 grd((ubh.nk() + 31) / 32, (ubh.nj() + 7) / 8, ubh.ni());
+      k_bulk_h<T><<<grd, blk, 0, s>>>(g, bh[0], bh[1], bh[2], ubh);
+      launches++;
+    }
+    if (nsibc && ntgt) {
+      k_sibc_h<T><<<blocks_for(ntgt, 128), 128, 0, s>>>(g, d_tgt_index, d_tgt_comp, d_tgt_start, ntgt, d_ops, d_etan);
+      launches++;
+    }
+    for (auto &l : srcs)
+      if (l.c > EZ) {
+        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, 0);
+        launches++;
+      }
+    for (auto &w : pws) {
+      if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
+      if (w.total_h) {
+        k_tfsf<T><<<blocks_for(w.total_h, 128), 128, 0, s>>>(g, w.pv, w.th, w.total_h, p.dt, d_step, 0, 0);
+        launches++;
+      }
+    }
+    if (ghost_h) {
+      k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 12), 128, 0, s>>>(g, gv, 0, 0);
+      launches++;
+    }
+    k_advance<<<1, 1, 0, s>>>(d_step);
+    launches++;
+    launches_per_step = launches;
+    return 0;
+  }
+
+  int capture_graph()
+  {
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int q = 0; q < kChunk; q++) enqueue_step();
+    CK(cudaStreamEndCapture(s, &gr));
+    cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return set_err(VGPU_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    return 0;
+  }
+
+  // Accumulate the DFT of output rows [r0, r1) (one chunk at most).
+  int dft_rows(uint64_t r0, uint64_t r1)
+  {
+    if (!p.num_fd || r1 <= r0) return 0;
+    int nrows = (int)(r1 - r0);
+    int nf = p.num_freq, npc = p.num_fd * 6;
+    k_twiddle<<<blocks_for((int64_t)nrows * nf, 128), 128, 0, s>>>(d_omega, nf, p.dt, p.out_start, r0, nrows, d_tw);
+    dim3 blk(32, 8), grd((nf + 31) / 32, (npc + 7) / 8);
+    size_t shm = sizeof(double) * 8 * nrows;
+    k_dft_accumulate<<<grd, blk, shm, s>>>(d_stage, npc, nf, nrows, (int)(r0 % kTB), kTB, d_tw, d_re, d_im);
+    stats.kernel_launches += 2;
+    return 0;
+  }
+
+  int run(uint64_t nsteps) override
+  {
+    if (step + nsteps > p.num_steps)
+      return set_err(VGPU_EINVAL, "run of %llu steps from step %llu exceeds the problem's %llu steps",
+                     (unsigned long long)nsteps, (unsigned long long)step, (unsigned long long)p.num_steps);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    uint64_t done = 0, launches = 0;
+    stats.kernel_launches = 0;
+    while (done < nsteps) {
+      uint64_t n0 = step;
+      // Chunks stay aligned so the DFT staging rows of one chunk never wrap.
+      uint64_t room = kChunk - (n0 % kChunk);
+      uint64_t m = std::min<uint64_t>(room, nsteps - done);
+      if (m == (uint64_t)kChunk) {
+        CK(cudaGraphLaunch(graph, s));
+      } else {
+        for (uint64_t q = 0; q < m; q++) enqueue_step();
+      }
+      launches += m * launches_per_step;
+      step += m;
+      done += m;
+      // Output rows produced in this chunk.
+      uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
+      if (p.num_fd && hi >= lo) {
+        if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
+      }
+    }
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stats.run_ms = ms;
+    stats.steps = nsteps;
+    stats.kernel_launches += launches;
+    return 0;
+  }
+
+  int read_td(double *out, uint64_t steps) override
+  {
+    size_t n = (size_t)std::min<uint64_t>(steps, nout) * p.num_td * 6;
+    std::vector<T> tmp(n ? n : 1);
+    if (n) CK(cudaMemcpy(tmp.data(), d_td, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < n; q++) out[q] = (double)tmp[q];
+    return 0;
+  }
+
+  int read_dft(double *re, double *im) override
+  {
+    size_t n = (size_t)p.num_fd * 6 * p.num_freq;
+    if (!n) return 0;
+    CK(cudaMemcpy(re, d_re, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(im, d_im, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return 0;
+  }
+
+  int read_field(int c, double *out) override
+  {
+    std::vector<T> tmp((size_t)vol);
+    CK(cudaMemcpy(tmp.data(), g.F[c], sizeof(T) * vol, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < p.n[0]; i++)
+      for (int j = 0; j < p.n[1]; j++)
+        for (int k = 0; k < p.n[2]; k++)
+          out[((int64_t)i * p.n[1] + j) * p.n[2] + k] = (double)tmp[(int64_t)i * g.s0 + (int64_t)j * g.s1 + k];
+    return 0;
+  }
+
+  int write_field(int c, const double *in) override
+  {
+    CK(cudaStreamSynchronize(s));
+    return upload_volume(g.F[c], in);
+  }
+
+  int check_finite() override
+  {
+    int *flag;
+    if (mem.alloc(&flag, 1)) return VGPU_ENOMEM;
+    CK(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    k_finite<T><<<592, 256, 0, s>>>(g, vol, flag);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h ? set_err(VGPU_ENONFINITE, "non-finite field value found") : 0;
+  }
+};
+
+struct vgpu_engine {
+  EngineBase *impl;
+};
+
+static int validate(const vgpu_problem *p)
+{
+  if (!p) return set_err(VGPU_EINVAL, "null problem");
+  if (p->abi_version != VGPU_ABI_VERSION) return set_err(VGPU_EINVAL, "ABI version %d, expected %d", p->abi_version, VGPU_ABI_VERSION);
+  if (p->precision != VGPU_FP64 && p->precision != VGPU_FP32) return set_err(VGPU_EINVAL, "invalid precision %d", p->precision);
+  for (int a = 0; a < 3; a++)
+    if (p->n[a] < 3) return set_err(VGPU_EINVAL, "grid extent n[%d]=%d too small", a, p->n[a]);
+  for (int q = 0; q < 9; q++)
+    if (!p->coef[q]) return set_err(VGPU_EINVAL, "coefficient volume %d missing", q);
+  for (int a = 0; a < 3; a++)
+    if (!p->ide[a] || !p->idh[a]) return set_err(VGPU_EINVAL, "edge length arrays missing");
+  // Every limit used by an update must keep its stencil inside the volume:
+  // E updates read the -1 neighbours, H updates the +1 neighbours.
+  auto in_grid = [&](const int32_t l[6], int field) {
+    if (l[1] < l[0] || l[3] < l[2] || l[5] < l[4]) return true;
+    int lo = field <= 2 ? 1 : 0, hi_off = field <= 2 ? 1 : 2;
+    for (int a = 0; a < 3; a++)
+      if (l[2 * a] < lo || l[2 * a + 1] > p->n[a] - hi_off) return false;
+    return true;
+  };
+  for (int f = 0; f < 6; f++)
+    if (!in_grid(p->gfilim[f], f)) return set_err(VGPU_EINVAL, "bulk limits of field %d outside the grid", f);
+  for (int r = 0; r < 6; r++)
+    if (p->pml_present[r])
+      for (int f = 0; f < 6; f++)
+        if (!in_grid(p->pml_flim[r][f], f)) return set_err(VGPU_EINVAL, "PML limits outside the grid");
+  for (int q = 0; q < p->num_sources; q++) {
+    const int32_t *l = p->sources[q].flim;
+    if (!(l[1] < l[0] || l[3] < l[2] || l[5] < l[4]) &&
+        (l[0] < 0 || l[2] < 0 || l[4] < 0 || l[1] >= p->n[0] || l[3] >= p->n[1] || l[5] >= p->n[2]))
+      return set_err(VGPU_EINVAL, "source %d limits outside the grid", q);
+    if (p->num_steps && !p->sources[q].values) return set_err(VGPU_EINVAL, "source %d has no values", q);
+  }
+  for (int q = 0; q < p->num_td; q++)
+    for (int a = 0; a < 3; a++)
+      if (p->td_points[3 * q + a] < 0 || p->td_points[3 * q + a] >= p->n[a]) return set_err(VGPU_EINVAL, "observer point outside the grid");
+  for (int q = 0; q < p->num_fd; q++)
+    for (int a = 0; a < 3; a++)
+      if (p->fd_points[3 * q + a] < 0 || p->fd_points[3 * q + a] >= p->n[a]) return set_err(VGPU_EINVAL, "observer point outside the grid");
+  return 0;
+}
+
+extern "C" int vgpu_create(const vgpu_problem *p, vgpu_engine **out)
+{
+  if (!out) return set_err(VGPU_EINVAL, "null output pointer");
+  *out = nullptr;
+  if (int rc = validate(p)) return rc;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return set_err(VGPU_ENODEV, "no CUDA device: %s", cudaGetErrorString(e));
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  if (prop.major != 10) return set_err(VGPU_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a", dev, prop.major, prop.minor);
+  EngineBase *impl = nullptr;
+  int rc;
+  if (p->precision == VGPU_FP64) {
+    auto *en = new Engine<double>();
+    rc = en->create(p);
+    impl = en;
+  } else {
+    auto *en = new Engine<float>();
+    rc = en->create(p);
+    impl = en;
+  }
+  if (rc) {
+    delete impl;
+    return rc;
+  }
+  *out = new vgpu_engine{ impl };
+  return 0;
+}
+
+extern "C" int vgpu_run(vgpu_engine *e, uint64_t nsteps)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  return e->impl->run(nsteps);
+}
+
+extern "C" int vgpu_read_td(vgpu_engine *e, double *out, uint64_t steps)
+{
+  if (!e || !out) return set_err(VGPU_EINVAL, "null argument");
+  return e->impl->read_td(out, steps);
+}
+
+extern "C" int vgpu_read_dft(vgpu_engine *e, double *re, double *im)
+{
+  if (!e || !re || !im) return set_err(VGPU_EINVAL, "null argument");
+  return e->impl->read_dft(re, im);
+}
+
+extern "C" int vgpu_read_field(vgpu_engine *e, int32_t c, double *out)
+{
+  if (!e || !out || c < 0 || c > 5) return set_err(VGPU_EINVAL, "invalid argument");
+  return e->impl->read_field(c, out);
+}
+
+extern "C" int vgpu_write_field(vgpu_engine *e, int32_t c, const double *in)
+{
+  if (!e || !in || c < 0 || c > 5) return set_err(VGPU_EINVAL, "invalid argument");
+  return e->impl->write_field(c, in);
+}
+
+extern "C" int vgpu_check_finite(vgpu_engine *e)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  return e->impl->check_finite();
+}
+
+extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
+
+extern "C" int vgpu_get_stats(const vgpu_engine *e, vgpu_stats *st)
+{
+  if (!e || !st) return set_err(VGPU_EINVAL, "null argument");
+  *st = e->impl->stats;
+  return 0;
+}
+
+extern "C" void vgpu_destroy(vgpu_engine *e)
+{
+  if (!e) return;
+  delete e->impl;
+  delete e;
+}

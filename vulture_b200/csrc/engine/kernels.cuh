@@ -1,0 +1,835 @@
+// kernels.cuh -- device kernels of the vulture_b200 FDTD engine (sm_100a).
+//
+// Every kernel restates one update routine of the reference time loop
+// (src/simulation.c:156-222) with the same arithmetic expressions in the same
+// order; the engine is built with --fmad=false so that in FP64 each value is
+// bit-identical to the reference's real=double solver.  T is the storage and
+// arithmetic type of fields and coefficients (double or float); DFT
+// accumulators, Debye currents, SIBC filter state and the analytic incident
+// field phase are always double.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vgpu.h"
+
+namespace vgpu_dev {
+
+enum { EX = 0, EY, EZ, HX, HY, HZ };
+
+// Inclusive index box.
+struct Box {
+  int i0, i1, j0, j1, k0, k1;
+  __host__ __device__ bool contains(int i, int j, int k) const {
+    return i >= i0 && i <= i1 && j >= j0 && j <= j1 && k >= k0 && k <= k1;
+  }
+  __host__ __device__ int ni() const { return i1 - i0 + 1; }
+  __host__ __device__ int nj() const { return j1 - j0 + 1; }
+  __host__ __device__ int nk() const { return k1 - k0 + 1; }
+  __host__ __device__ bool empty() const { return i1 < i0 || j1 < j0 || k1 < k0; }
+  __host__ __device__ int64_t count() const { return empty() ? 0 : (int64_t)ni() * nj() * nk(); }
+};
+
+static inline Box box_from(const int32_t l[6]) { return Box{ l[0], l[1], l[2], l[3], l[4], l[5] }; }
+
+// Device view of the grid: fields, coefficients and line arrays.  Volumes are
+// [n0][n1][n2p] with the k rows padded to a multiple of 32 elements.
+template <typename T>
+struct Grid {
+  T *F[6];
+  const T *cf[9];
+  const T *ide[3];
+  const T *idh[3];
+  int n0, n1, n2;
+  int64_t s0, s1;  // strides of i and j
+  __device__ __forceinline__ int64_t at(int i, int j, int k) const { return (int64_t)i * s0 + (int64_t)j * s1 + k; }
+};
+
+// ---------------------------------------------------------------------------
+// Bulk Yee updates (src/grid.c:709-888): one thread per (i,j,k) of the union
+// of the three components' limits, each component guarded by its own box.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_bulk_e(Grid<T> g, Box bx, Box by, Box bz, Box uni)
+{
+  int k = uni.k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = uni.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int i = uni.i0 + blockIdx.z;
+  if (k > uni.k1 || j > uni.j1) return;
+  const int64_t x = g.at(i, j, k);
+  T *__restrict__ Ex = g.F[EX];
+  T *__restrict__ Ey = g.F[EY];
+  T *__restrict__ Ez = g.F[EZ];
+  const T *__restrict__ Hx = g.F[HX];
+  const T *__restrict__ Hy = g.F[HY];
+  const T *__restrict__ Hz = g.F[HZ];
+  if (bx.contains(i, j, k))
+    Ex[x] = g.cf[0][x] * Ex[x] + g.cf[3][x] * (g.idh[1][j] * (Hz[x] - Hz[x - g.s1]) + g.idh[2][k] * (Hy[x - 1] - Hy[x]));
+  if (by.contains(i, j, k))
+    Ey[x] = g.cf[1][x] * Ey[x] + g.cf[4][x] * (g.idh[2][k] * (Hx[x] - Hx[x - 1]) + g.idh[0][i] * (Hz[x - g.s0] - Hz[x]));
+  if (bz.contains(i, j, k))
+    Ez[x] = g.cf[2][x] * Ez[x] + g.cf[5][x] * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
+}
+
+template <typename T>
+__global__ void k_bulk_h(Grid<T> g, Box bx, Box by, Box bz, Box uni)
+{
+  int k = uni.k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = uni.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int i = uni.i0 + blockIdx.z;
+  if (k > uni.k1 || j > uni.j1) return;
+  const int64_t x = g.at(i, j, k);
+  const T *__restrict__ Ex = g.F[EX];
+  const T *__restrict__ Ey = g.F[EY];
+  const T *__restrict__ Ez = g.F[EZ];
+  T *__restrict__ Hx = g.F[HX];
+  T *__restrict__ Hy = g.F[HY];
+  T *__restrict__ Hz = g.F[HZ];
+  if (bx.contains(i, j, k))
+    Hx[x] = Hx[x] + g.cf[6][x] * (g.ide[2][k] * (Ey[x + 1] - Ey[x]) + g.ide[1][j] * (Ez[x] - Ez[x + g.s1]));
+  if (by.contains(i, j, k))
+    Hy[x] = Hy[x] + g.cf[7][x] * (g.ide[0][i] * (Ez[x + g.s0] - Ez[x]) + g.ide[2][k] * (Ex[x] - Ex[x + 1]));
+  if (bz.contains(i, j, k))
+    Hz[x] = Hz[x] + g.cf[8][x] * (g.ide[1][j] * (Ex[x + g.s1] - Ex[x]) + g.ide[0][i] * (Ey[x] - Ey[x + g.s0]));
+}
+
+// ---------------------------------------------------------------------------
+// UPML (src/pml.c:859-1176).  All present regions in one launch: blockIdx.z
+// runs over the concatenated i-planes of the regions' union boxes.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct PmlView {
+  const T *ad[3], *bd[3], *ah[3], *bh[3], *ibd[3], *ibh[3];
+  int nreg;
+  int reg_plane0[7];   // first blockIdx.z of each region
+  Box uni[6];          // union box of the region's three components
+  Box lim[6][6];       // [region][field]
+  T *PP[6][3], *P[6][3], *B[6][3];
+};
+
+__device__ __forceinline__ int64_t aux_index(const Box &l, int i, int j, int k)
+{
+  return ((int64_t)(i - l.i0) * l.nj() + (j - l.j0)) * l.nk() + (k - l.k0);
+}
+
+template <typename T>
+__global__ void k_pml_e(Grid<T> g, PmlView<T> pv)
+{
+  int z = blockIdx.z, r = 0;
+  while (r + 1 < pv.nreg && z >= pv.reg_plane0[r + 1]) r++;
+  const Box u = pv.uni[r];
+  int i = u.i0 + (z - pv.reg_plane0[r]);
+  int j = u.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int k = u.k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > u.k1 || j > u.j1) return;
+  const int64_t x = g.at(i, j, k);
+  const T *Hx = g.F[HX], *Hy = g.F[HY], *Hz = g.F[HZ];
+  {
+    const Box &l = pv.lim[r][EX];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *PP = pv.PP[r][0], *P = pv.P[r][0];
+      T oPP = PP[a];
+      PP[a] = g.cf[0][x] * PP[a] + g.cf[3][x] * (g.idh[1][j] * (Hz[x] - Hz[x - g.s1]) + g.idh[2][k] * (Hy[x - 1] - Hy[x]));
+      T oP = P[a];
+      P[a] = pv.ad[1][j] * P[a] + pv.bd[1][j] * (PP[a] - oPP);
+      g.F[EX][x] = pv.ad[2][k] * g.F[EX][x] + pv.bd[2][k] * pv.ibh[0][i] * (P[a] - pv.ah[0][i] * oP);
+    }
+  }
+  {
+    const Box &l = pv.lim[r][EY];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *PP = pv.PP[r][1], *P = pv.P[r][1];
+      T oPP = PP[a];
+      PP[a] = g.cf[1][x] * PP[a] + g.cf[4][x] * (g.idh[2][k] * (Hx[x] - Hx[x - 1]) + g.idh[0][i] * (Hz[x - g.s0] - Hz[x]));
+      T oP = P[a];
+      P[a] = pv.ad[2][k] * P[a] + pv.bd[2][k] * (PP[a] - oPP);
+      g.F[EY][x] = pv.ad[0][i] * g.F[EY][x] + pv.bd[0][i] * pv.ibh[1][j] * (P[a] - pv.ah[1][j] * oP);
+    }
+  }
+  {
+    const Box &l = pv.lim[r][EZ];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *PP = pv.PP[r][2], *P = pv.P[r][2];
+      T oPP = PP[a];
+      PP[a] = g.cf[2][x] * PP[a] + g.cf[5][x] * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
+      T oP = P[a];
+      P[a] = pv.ad[0][i] * P[a] + pv.bd[0][i] * (PP[a] - oPP);
+      g.F[EZ][x] = pv.ad[1][j] * g.F[EZ][x] + pv.bd[1][j] * pv.ibh[2][k] * (P[a] - pv.ah[2][k] * oP);
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_pml_h(Grid<T> g, PmlView<T> pv)
+{
+  int z = blockIdx.z, r = 0;
+  while (r + 1 < pv.nreg && z >= pv.reg_plane0[r + 1]) r++;
+  const Box u = pv.uni[r];
+  int i = u.i0 + (z - pv.reg_plane0[r]);
+  int j = u.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int k = u.k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > u.k1 || j > u.j1) return;
+  const int64_t x = g.at(i, j, k);
+  const T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
+  {
+    const Box &l = pv.lim[r][HX];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *B = pv.B[r][0];
+      T oB = B[a];
+      B[a] = pv.ah[1][j] * B[a] + g.cf[6][x] * pv.bh[1][j] * (g.ide[2][k] * (Ey[x + 1] - Ey[x]) + g.ide[1][j] * (Ez[x] - Ez[x + g.s1]));
+      g.F[HX][x] = pv.ah[2][k] * g.F[HX][x] + pv.bh[2][k] * pv.ibd[0][i] * (B[a] - pv.ad[0][i] * oB);
+    }
+  }
+  {
+    const Box &l = pv.lim[r][HY];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *B = pv.B[r][1];
+      T oB = B[a];
+      B[a] = pv.ah[2][k] * B[a] + g.cf[7][x] * pv.bh[2][k] * (g.ide[0][i] * (Ez[x + g.s0] - Ez[x]) + g.ide[2][k] * (Ex[x] - Ex[x + 1]));
+      g.F[HY][x] = pv.ah[0][i] * g.F[HY][x] + pv.bh[0][i] * pv.ibd[1][j] * (B[a] - pv.ad[1][j] * oB);
+    }
+  }
+  {
+    const Box &l = pv.lim[r][HZ];
+    if (l.contains(i, j, k)) {
+      int64_t a = aux_index(l, i, j, k);
+      T *B = pv.B[r][2];
+      T oB = B[a];
+      B[a] = pv.ah[0][i] * B[a] + g.cf[8][x] * pv.bh[0][i] * (g.ide[1][j] * (Ex[x + g.s1] - Ex[x]) + g.ide[0][i] * (Ey[x] - Ey[x + g.s0]));
+      g.F[HZ][x] = pv.ah[1][j] * g.F[HZ][x] + pv.bh[1][j] * pv.ibd[2][k] * (B[a] - pv.ad[2][k] * oB);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mur first-order ABC (src/mur.c:135-555).  A list of planar work items; each
+// thread updates one tangential E (before the bulk update, reading the
+// neighbour's pre-update value) or one normal H.
+// ---------------------------------------------------------------------------
+
+struct MurItem {
+  Box b;            // the face plane for component c
+  int c;            // field component
+  int axis, dir;    // neighbour offset along axis (E items)
+  int face;
+  int64_t first;    // first flattened thread of the item
+};
+
+struct MurView {
+  int nitems;
+  MurItem it[12];
+  double zeta[6];
+};
+
+template <typename T>
+__device__ __forceinline__ T bulk_e_value(const Grid<T> &g, int c, int i, int j, int k)
+{
+  const int64_t x = g.at(i, j, k);
+  const T *Hx = g.F[HX], *Hy = g.F[HY], *Hz = g.F[HZ];
+  if (c == EX) return g.cf[0][x] * g.F[EX][x] + g.cf[3][x] * (g.idh[1][j] * (Hz[x] - Hz[x - g.s1]) + g.idh[2][k] * (Hy[x - 1] - Hy[x]));
+  if (c == EY) return g.cf[1][x] * g.F[EY][x] + g.cf[4][x] * (g.idh[2][k] * (Hx[x] - Hx[x - 1]) + g.idh[0][i] * (Hz[x - g.s0] - Hz[x]));
+  return g.cf[2][x] * g.F[EZ][x] + g.cf[5][x] * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
+}
+
+template <typename T>
+__device__ __forceinline__ void item_coords(const MurItem &m, int64_t t, int &i, int &j, int &k)
+{
+  int64_t nj = m.b.nj(), nk = m.b.nk();
+  i = m.b.i0 + (int)(t / (nj * nk));
+  j = m.b.j0 + (int)((t / nk) % nj);
+  k = m.b.k0 + (int)(t % nk);
+}
+
+template <typename T>
+__global__ void k_mur_e(Grid<T> g, MurView mv, int64_t total)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int q = 0;
+  while (q + 1 < mv.nitems && t >= mv.it[q + 1].first) q++;
+  const MurItem &m = mv.it[q];
+  int i, j, k;
+  item_coords<T>(m, t - m.first, i, j, k);
+  int n[3] = { i, j, k };
+  n[m.axis] += m.dir;
+  T tmp = bulk_e_value(g, m.c, n[0], n[1], n[2]);
+  int64_t x = g.at(i, j, k), xn = g.at(n[0], n[1], n[2]);
+  T *F = g.F[m.c];
+  F[x] = F[xn] + (T)mv.zeta[m.face] * (tmp - F[x]);
+}
+
+template <typename T>
+__global__ void k_mur_h(Grid<T> g, MurView mv, int64_t total)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int q = 0;
+  while (q + 1 < mv.nitems && t >= mv.it[q + 1].first) q++;
+  const MurItem &m = mv.it[q];
+  int i, j, k;
+  item_coords<T>(m, t - m.first, i, j, k);
+  const int64_t x = g.at(i, j, k);
+  const T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
+  if (m.c == HX)
+    g.F[HX][x] = g.F[HX][x] + g.cf[6][x] * (g.ide[2][k] * (Ey[x + 1] - Ey[x]) + g.ide[1][j] * (Ez[x] - Ez[x + g.s1]));
+  else if (m.c == HY)
+    g.F[HY][x] = g.F[HY][x] + g.cf[7][x] * (g.ide[0][i] * (Ez[x + g.s0] - Ez[x]) + g.ide[2][k] * (Ex[x] - Ex[x + 1]));
+  else
+    g.F[HZ][x] = g.F[HZ][x] + g.cf[8][x] * (g.ide[1][j] * (Ex[x + g.s1] - Ex[x]) + g.ide[0][i] * (Ey[x] - Ey[x + g.s0]));
+}
+
+// ---------------------------------------------------------------------------
+// Debye blocks (src/debye.c:243-307): one thread per (block, component, cell).
+// ---------------------------------------------------------------------------
+
+struct DebyeItem {
+  Box b;
+  int c, np;
+  int64_t first;     // first flattened thread
+  int64_t jofs;      // offset of this item's currents (complex) in J
+  int64_t eofs;      // offset of this item's cells in lastE
+  int coef_ofs;      // offset of dalpha/dbeta (complex, np each) in coefs
+};
+
+template <typename T>
+__global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t total, double2 *J, T *lastE,
+                        const double2 *coefs)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int q = 0;
+  while (q + 1 < nitems && t >= items[q + 1].first) q++;
+  const DebyeItem m = items[q];
+  int64_t cell = t - m.first;
+  int64_t nj = m.b.nj(), nk = m.b.nk();
+  int i = m.b.i0 + (int)(cell / (nj * nk)), j = m.b.j0 + (int)((cell / nk) % nj), k = m.b.k0 + (int)(cell % nk);
+  const int64_t x = g.at(i, j, k);
+  T *E = g.F[m.c];
+  const double2 *da = coefs + m.coef_ofs, *db = da + m.np;
+  double2 *Jc = J + m.jofs + cell * m.np;
+  // Jsum = sum (1 + dalpha) * J, complex arithmetic as C99 (no contraction).
+  double sr = 0.0, si = 0.0;
+  for (int p = 0; p < m.np; p++) {
+    double ar = 1 + da[p].x, ai = da[p].y;
+    double2 v = Jc[p];
+    sr = sr + (ar * v.x - ai * v.y);
+    si = si + (ar * v.y + ai * v.x);
+  }
+  E[x] = E[x] - g.cf[3 + m.c][x] * sr;
+  T diff = E[x] - lastE[m.eofs + cell];
+  for (int p = 0; p < m.np; p++) {
+    double2 v = Jc[p];
+    double nr = (da[p].x * v.x - da[p].y * v.y) + db[p].x * (double)diff;
+    double ni = (da[p].x * v.y + da[p].y * v.x) + db[p].y * (double)diff;
+    Jc[p] = make_double2(nr, ni);
+  }
+  lastE[m.eofs + cell] = E[x];
+}
+
+// ---------------------------------------------------------------------------
+// Sources (src/source.c:602-753).
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_source(Grid<T> g, Box b, int c, int kind, T soft, const T *values, const uint64_t *step_base,
+                         int step_rel)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b.count()) return;
+  int64_t nj = b.nj(), nk = b.nk();
+  int i = b.i0 + (int)(t / (nj * nk)), j = b.j0 + (int)((t / nk) % nj), k = b.k0 + (int)(t % nk);
+  const int64_t x = g.at(i, j, k);
+  T v = values[*step_base + step_rel];
+  T *F = g.F[c];
+  if (kind == VGPU_SRC_FIELD) F[x] = soft * F[x] + v;
+  else F[x] = soft * F[x] - g.cf[c <= EZ ? 3 + c : 6 + c - HX][x] * v;
+}
+
+// ---------------------------------------------------------------------------
+// Ghost layer (src/surface.c:569-812).  One launch per field type.  E: each
+// component belongs to one axis.  H: each component is written by the faces of
+// two axes in the reference's order (X, Y, Z); a point on two ghost planes
+// takes the composition of both copies, which equals the reference's
+// sequential result because every copy reads interior values.
+// ---------------------------------------------------------------------------
+
+struct GhostView {
+  int mode[6];        // VGPU_GHOST_* per face
+  int go_lo[3], go_hi[3];
+};
+
+__device__ __forceinline__ bool ghost_src(const GhostView &gv, int axis, int idx, int &src, int &neg)
+{
+  int lo = gv.go_lo[axis], hi = gv.go_hi[axis];
+  int face;
+  if (idx == lo - 1) face = 2 * axis;
+  else if (idx == hi) face = 2 * axis + 1;
+  else return false;
+  int mode = gv.mode[face];
+  if (mode == VGPU_GHOST_NONE) return false;
+  bool is_lo = (face % 2) == 0;
+  if (mode == VGPU_GHOST_PERIODIC) src = is_lo ? hi - 1 : lo;
+  else src = is_lo ? lo : hi - 1;
+  neg = mode == VGPU_GHOST_PMC;
+  return true;
+}
+
+template <typename T>
+__global__ void k_ghost(Grid<T> g, GhostView gv, int efield, int nb_all)
+{
+  // blockIdx.y: which (component, axis, side) plane; threads: points on it.
+  int plane = blockIdx.y;
+  int comp, axis, side;
+  if (efield) {
+    axis = plane / 2;
+    side = plane % 2;
+    comp = axis;
+  } else {
+    // H: 3 components x 2 writer axes x 2 sides.
+    comp = HX + plane / 4;
+    int w = (plane / 2) % 2;
+    int ca = comp - HX;
+    axis = (w == 0) ? (ca == 0 ? 1 : 0) : (ca == 2 ? 1 : 2);
+    side = plane % 2;
+  }
+  int face = 2 * axis + side;
+  if (gv.mode[face] == VGPU_GHOST_NONE) return;
+  int b = (axis + 1) % 3, c = (axis + 2) % 3;
+  int nbp = gv.go_hi[b] - gv.go_lo[b] + 2, ncp = gv.go_hi[c] - gv.go_lo[c] + 2;
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nbp * ncp) return;
+  int ib = gv.go_lo[b] - 1 + (int)(t / ncp), ic = gv.go_lo[c] - 1 + (int)(t % ncp);
+  int p[3];
+  p[axis] = side == 0 ? gv.go_lo[axis] - 1 : gv.go_hi[axis];
+  p[b] = ib;
+  p[c] = ic;
+  T *F = g.F[comp];
+  if (efield) {
+    int src, neg;
+    ghost_src(gv, axis, p[axis], src, neg);
+    int s[3] = { p[0], p[1], p[2] };
+    s[axis] = src;
+    T v = F[g.at(s[0], s[1], s[2])];
+    F[g.at(p[0], p[1], p[2])] = neg ? -v : v;
+    return;
+  }
+  // H: the writer axes of comp, in reference order.
+  int ca = comp - HX;
+  int A = ca == 0 ? 1 : 0;          // first writer axis
+  int Bx = ca == 2 ? 1 : 2;         // second writer axis
+  int srcA, negA, srcB, negB;
+  bool onA = ghost_src(gv, A, p[A], srcA, negA);
+  bool onB = ghost_src(gv, Bx, p[Bx], srcB, negB);
+  // A point on both planes is handled by the thread of the later axis only.
+  if (axis == A && onB) return;
+  int s[3] = { p[0], p[1], p[2] };
+  bool neg = false;
+  if (onB) { s[Bx] = srcB; neg = negB; }
+  if (onA) { s[A] = srcA; neg = neg != (bool)negA; }
+  T v = F[g.at(s[0], s[1], s[2])];
+  F[g.at(p[0], p[1], p[2])] = neg ? -v : v;
+  (void)nb_all;
+}
+
+// ---------------------------------------------------------------------------
+// Observers (src/observer.c:622-650, 857-899).
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_observe(Grid<T> g, const int *td_pts, int num_td, const int *fd_pts, int num_fd, T *td_buf,
+                          double *fd_stage, const uint64_t *step_base, int step_rel, uint64_t out_start,
+                          uint64_t out_stop, int tblock)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t n = *step_base + step_rel;
+  if (n < out_start || n > out_stop) return;
+  uint64_t row = n - out_start;
+  if (t < num_td * 6) {
+    int p = t / 6, c = t % 6;
+    const int *pt = td_pts + 3 * p;
+    td_buf[(row * num_td + p) * 6 + c] = g.F[c][g.at(pt[0], pt[1], pt[2])];
+    return;
+  }
+  t -= num_td * 6;
+  if (t < num_fd * 6) {
+    int p = t / 6, c = t % 6;
+    const int *pt = fd_pts + 3 * p;
+    fd_stage[(row % tblock) * (int64_t)num_fd * 6 + t] = (double)g.F[c][g.at(pt[0], pt[1], pt[2])];
+  }
+}
+
+// Twiddles cos/sin(omega_f * t_n) for the rows of one DFT block.
+__global__ void k_twiddle(const double *omega, int nf, double dt, uint64_t out_start, uint64_t row0, int nrows,
+                          double2 *tw)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows * nf) return;
+  int r = t / nf, f = t % nf;
+  double time = (double)(out_start + row0 + r) * dt;
+  double wt = omega[f] * time;
+  double s, c;
+  sincos(wt, &s, &c);
+  tw[t] = make_double2(c, s);
+}
+
+// re[pc][f] += v*cos, im[pc][f] -= v*sin for each buffered row in order, one
+// thread per (pc, f): the same sequence of additions as the reference's
+// per-step accumulation.
+__global__ void k_dft_accumulate(const double *stage, int npc, int nf, int nrows, int row_offset, int tblock,
+                                 const double2 *tw, double *re, double *im)
+{
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int pc = blockIdx.y * blockDim.y + threadIdx.y;
+  extern __shared__ double sm[];
+  double *vs = sm;  // [blockDim.y][nrows]
+  for (int q = threadIdx.y * blockDim.x + threadIdx.x; q < blockDim.y * nrows; q += blockDim.x * blockDim.y) {
+    int py = q / nrows, r = q % nrows;
+    int pcq = blockIdx.y * blockDim.y + py;
+    vs[q] = pcq < npc ? stage[((row_offset + r) % tblock) * (int64_t)npc + pcq] : 0.0;
+  }
+  __syncthreads();
+  if (f >= nf || pc >= npc) return;
+  double ar = re[(int64_t)pc * nf + f], ai = im[(int64_t)pc * nf + f];
+  const double *v = vs + threadIdx.y * nrows;
+  for (int r = 0; r < nrows; r++) {
+    double2 w = tw[(int64_t)r * nf + f];
+    ar = ar + v[r] * w.x;
+    ai = ai - v[r] * w.y;
+  }
+  re[(int64_t)pc * nf + f] = ar;
+  im[(int64_t)pc * nf + f] = ai;
+}
+
+// ---------------------------------------------------------------------------
+// Waveforms on the device (src/waveform.c:412-638), used by the analytic
+// plane-wave incident field.  Evaluated in double.
+// ---------------------------------------------------------------------------
+
+struct DevWaveform {
+  int type, table_size;
+  double size, delay, width, frequency;
+  const double *table;
+};
+
+__device__ inline double dev_spline(const DevWaveform &w, double t)
+{
+  const double *tab = w.table;
+  unsigned long n = (unsigned long)w.table_size, klo = 0, khi = n - 1, k;
+  while (khi - klo > 1UL) {
+    k = (khi + klo) >> 1;
+    if (tab[3 * k] > t) khi = k;
+    else klo = k;
+  }
+  double h = tab[3 * khi] - tab[3 * klo];
+  double a = (tab[3 * khi] - t) / h, b = (t - tab[3 * klo]) / h;
+  return a * tab[3 * klo + 1] + b * tab[3 * khi + 1] +
+         ((a * a * a - a) * tab[3 * klo + 2] + (b * b * b - b) * tab[3 * khi + 2]) * (h * h) / 6.0;
+}
+
+__device__ inline double dev_waveform(const DevWaveform &w, double t, double delay)
+{
+  const double pi = 3.14159265358979311600;  // 4*atan(1) in double
+  double x = t - delay - w.delay, W = w.width, f = w.frequency, env;
+  switch (w.type) {
+    case VGPU_WF_GAUSSIAN_PULSE:
+    case VGPU_WF_NARROW_GAUSSIAN_PULSE: return w.size * exp(-0.5 * (pow(x / W, 2.0)));
+    case VGPU_WF_DIFF_GAUSSIAN_PULSE: return w.size * (-x / W * exp(-0.5 * (pow(x / W, 2.0))));
+    case VGPU_WF_RICKER_WAVELET: return w.size * ((1.0 - pow(x / W, 2.0)) * exp(-0.5 * (pow(x / W, 2.0))));
+    case VGPU_WF_MOD_GAUSSIAN_PULSE: return w.size * (exp(-0.5 * (pow(x / W, 2.0))) * sin(2.0 * pi * f * x));
+    case VGPU_WF_COMPACT_PULSE:
+    case VGPU_WF_MOD_COMPACT_PULSE:
+      if (x <= 0.0) env = 0.0;
+      else if (x < 2.0 * W)
+        env = 1.0 / 32.0 * (10.0 - 15.0 * cos(pi / W * x) + 6.0 * cos(2.0 * pi / W * x) - cos(3.0 * pi / W * x));
+      else env = 0.0;
+      return w.type == VGPU_WF_COMPACT_PULSE ? w.size * env : w.size * (env * sin(2.0 * pi * f * x));
+    case VGPU_WF_DIFF_COMPACT_PULSE:
+      if (x <= 0.0 || x >= 2.0 * W) return w.size * 0.0;
+      return w.size * (1.0 / 32.0 * (15.0 * sin(pi / W * x) - 12.0 * sin(2.0 * pi / W * x) + 3.0 * sin(3.0 * pi / W * x)));
+    case VGPU_WF_RAMPED_SINUSOID:
+      if (x <= 0.0) env = 0.0;
+      else if (x < 1.0 * W)
+        env = 1.0 / 32.0 * (10.0 - 15.0 * cos(pi / W * x) + 6.0 * cos(2.0 * pi / W * x) - cos(3.0 * pi / W * x));
+      else env = 1.0;
+      return w.size * (env * sin(2.0 * pi * f * x));
+    case VGPU_WF_EXTERNAL:
+      if (x < w.table[0] || x > w.table[3 * (w.table_size - 1)]) return w.size * 0.0;
+      return w.size * dev_spline(w, x);
+    default: return 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TFSF plane waves (src/planewave.c:576-1007, 1226-1419).
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct PwView {
+  int use_aux;
+  DevWaveform wf;
+  double delay, phase_velocity;
+  double kinc[3], finc[6], r0[3], ijk0[3];
+  const double *pos_node[3], *pos_half[3];
+  // auxiliary grid
+  T *Eyi, *Hzi, *PPyi, *Pyi, *Bzi;
+  const T *adx, *bdx, *ahx, *bhx;
+  const T *source;
+  int nx, xb;
+  T beta, gamma, eta0;
+};
+
+struct TfsfItem {
+  Box b;          // corrected points of this face for component c
+  int c, inc, sign, axis, shift;
+  int64_t first;
+};
+
+struct TfsfView {
+  int n;
+  TfsfItem it[12];
+};
+
+template <typename T>
+__device__ inline T incident_field(const PwView<T> &pw, int c, int i, int j, int k, double time)
+{
+  if (!pw.use_aux) {
+    int g[3] = { i, j, k };
+    double r[3];
+    for (int a = 0; a < 3; a++) {
+      bool half = c <= EZ ? (c == a) : (c - HX != a);
+      r[a] = half ? pw.pos_half[a][g[a]] : pw.pos_node[a][g[a]];
+    }
+    double d = pw.kinc[0] * (r[0] - pw.r0[0]) + pw.kinc[1] * (r[1] - pw.r0[1]) + pw.kinc[2] * (r[2] - pw.r0[2]);
+    return (T)(pw.finc[c] * dev_waveform(pw.wf, time - d / pw.phase_velocity, pw.delay));
+  }
+  T rc[3] = { (T)i, (T)j, (T)k };
+  if (c <= EZ) rc[c] = rc[c] + (T)0.5;
+  else
+    for (int a = 0; a < 3; a++)
+      if (a != c - HX) rc[a] = rc[a] + (T)0.5;
+  T d = (T)pw.kinc[0] * (rc[0] - (T)pw.ijk0[0]) + (T)pw.kinc[1] * (rc[1] - (T)pw.ijk0[1]) +
+        (T)pw.kinc[2] * (rc[2] - (T)pw.ijk0[2]);
+  T value;
+  if (c <= EZ) {
+    int id = (int)floor((double)d);
+    T dp = d - (T)id;
+    value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
+  } else {
+    int id = (int)floor((double)d + 0.5);
+    T dp = (T)((double)d + 0.5 - id);
+    value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
+  }
+  return (T)pw.finc[c] * value;
+}
+
+// Auxiliary 1-D grid, one block (src/planewave.c:1318-1374).
+template <typename T>
+__global__ void k_aux_e(PwView<T> pw, const uint64_t *step_base, int step_rel)
+{
+  for (int i = 1 + threadIdx.x; i < pw.xb; i += blockDim.x) pw.Eyi[i] = pw.Eyi[i] + pw.beta * (pw.Hzi[i - 1] - pw.Hzi[i]);
+  for (int i = pw.xb + threadIdx.x; i < pw.nx; i += blockDim.x) {
+    int L = i - pw.xb;
+    T oPP = pw.PPyi[L];
+    pw.PPyi[L] = pw.PPyi[L] + pw.beta * (pw.Hzi[i - 1] - pw.Hzi[i]);
+    T oP = pw.Pyi[L];
+    pw.Pyi[L] = pw.Pyi[L] + (pw.PPyi[L] - oPP);
+    pw.Eyi[i] = pw.adx[L] * pw.Eyi[i] + pw.bdx[L] * (pw.Pyi[L] - oP);
+  }
+  if (threadIdx.x == 0) pw.Eyi[0] = pw.source[*step_base + step_rel];
+}
+
+template <typename T>
+__global__ void k_aux_h(PwView<T> pw)
+{
+  for (int i = threadIdx.x; i < pw.xb; i += blockDim.x) pw.Hzi[i] = pw.Hzi[i] + pw.gamma * (pw.Eyi[i] - pw.Eyi[i + 1]);
+  for (int i = pw.xb + threadIdx.x; i < pw.nx; i += blockDim.x) {
+    int L = i - pw.xb;
+    T oB = pw.Bzi[L];
+    pw.Bzi[L] = pw.ahx[L] * pw.Bzi[L] + pw.gamma * pw.bhx[L] * (-pw.Eyi[i + 1] + pw.Eyi[i]);
+    pw.Hzi[i] = pw.Hzi[i] + (pw.Bzi[L] - oB);
+  }
+}
+
+// Face corrections.  A point on several faces (edges of the Huygens box) is
+// corrected by the thread of its first face, which applies all of its faces
+// in the reference's order (YLO, YHI, ZLO, ZHI, XLO, XHI).
+template <typename T>
+__global__ void k_tfsf(Grid<T> g, PwView<T> pw, TfsfView tv, int64_t total, double dt, const uint64_t *step_base,
+                       int step_rel, int efield)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int q = 0;
+  while (q + 1 < tv.n && t >= tv.it[q + 1].first) q++;
+  const TfsfItem &m = tv.it[q];
+  int64_t u = t - m.first, nj = m.b.nj(), nk = m.b.nk();
+  int i = m.b.i0 + (int)(u / (nj * nk)), j = m.b.j0 + (int)((u / nk) % nj), k = m.b.k0 + (int)(u % nk);
+  for (int e = 0; e < q; e++)
+    if (tv.it[e].c == m.c && tv.it[e].b.contains(i, j, k)) return;
+  uint64_t n = *step_base + step_rel;
+  double time = efield ? n * dt : (n + 0.5) * dt;
+  const int64_t x = g.at(i, j, k);
+  T *F = g.F[m.c];
+  for (int e = q; e < tv.n; e++) {
+    const TfsfItem &it = tv.it[e];
+    if (it.c != m.c || !it.b.contains(i, j, k)) continue;
+    int s[3] = { i, j, k };
+    s[it.axis] += it.shift;
+    T inc = incident_field(pw, it.inc, s[0], s[1], s[2], time);
+    int gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
+    if (efield) {
+      T al = g.cf[it.c][x], be = g.cf[3 + it.c][x], idv = g.idh[it.axis][gi];
+      if (it.sign > 0) F[x] = al * F[x] + be * (idv * inc);
+      else F[x] = al * F[x] - be * (idv * inc);
+    } else {
+      T ga = g.cf[6 + it.c - HX][x], idv = g.ide[it.axis][gi];
+      if (it.sign > 0) F[x] = F[x] + ga * (idv * inc);
+      else F[x] = F[x] - ga * (idv * inc);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SIBC (src/sibc.c:444-776, src/filter.c:309-327).
+// ---------------------------------------------------------------------------
+
+struct SibcSurf {
+  Box g;              // faces: cells [i0, i1) etc. stored as inclusive i0..i1-1
+  int normal, model;
+  int64_t first;      // first global face index
+  double A[4][4], B[4][4];
+};
+
+struct SibcModelDev {
+  int np[4][4], off[4][4];
+  double asymp[4][4];
+  int poles;          // total poles of the model
+};
+
+template <typename T>
+__global__ void k_sibc_e(Grid<T> g, const SibcSurf *surfs, int nsurf, const SibcModelDev *models,
+                         const double2 *q0, const double2 *q1, const double2 *q2, const uint8_t *adjA,
+                         const uint8_t *adjB, const int64_t *zofs, double2 *zeta, double *old, T *etan,
+                         int64_t total)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int s = 0;
+  while (s + 1 < nsurf && t >= surfs[s + 1].first) s++;
+  const SibcSurf &sf = surfs[s];
+  const SibcModelDev &m = models[sf.model];
+  int64_t f = t - sf.first;
+  int64_t nj = sf.g.nj(), nk = sf.g.nk();
+  int i = sf.g.i0 + (int)(f / (nj * nk)), j = sf.g.j0 + (int)((f / nk) % nj), k = sf.g.k0 + (int)(f % nk);
+  const uint8_t *A = adjA + 4 * t, *B = adjB + 4 * t;
+  T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
+  const T *Hx = g.F[HX], *Hy = g.F[HY], *Hz = g.F[HZ];
+  T Ht[4], Hin[4], Eout[4];
+  if (sf.normal == 0) {
+    Ey[g.at(i, j, k)] = 0.0; Ey[g.at(i, j, k + 1)] = 0.0;
+    Ez[g.at(i, j, k)] = 0.0; Ez[g.at(i, j + 1, k)] = 0.0;
+    Ht[0] = 0.5 * (1 + A[0] + A[1]) * (Hy[g.at(i - 1, j, k)] + Hy[g.at(i - 1, j + 1, k)]);
+    Ht[1] = 0.5 * (1 + B[0] + B[1]) * (Hy[g.at(i, j, k)] + Hy[g.at(i, j + 1, k)]);
+    Ht[2] = 0.5 * (1 + A[2] + A[3]) * (Hz[g.at(i - 1, j, k)] + Hz[g.at(i - 1, j, k + 1)]);
+    Ht[3] = 0.5 * (1 + B[2] + B[3]) * (Hz[g.at(i, j, k)] + Hz[g.at(i, j, k + 1)]);
+  } else if (sf.normal == 1) {
+    Ez[g.at(i, j, k)] = 0.0; Ez[g.at(i + 1, j, k)] = 0.0;
+    Ex[g.at(i, j, k)] = 0.0; Ex[g.at(i, j, k + 1)] = 0.0;
+    Ht[0] = 0.5 * (1 + A[0] + A[1]) * (Hz[g.at(i, j - 1, k)] + Hz[g.at(i, j - 1, k + 1)]);
+    Ht[1] = 0.5 * (1 + B[0] + B[1]) * (Hz[g.at(i, j, k)] + Hz[g.at(i, j, k + 1)]);
+    Ht[2] = 0.5 * (1 + A[2] + A[3]) * (Hx[g.at(i, j - 1, k)] + Hx[g.at(i + 1, j - 1, k)]);
+    Ht[3] = 0.5 * (1 + B[2] + B[3]) * (Hx[g.at(i, j, k)] + Hx[g.at(i + 1, j, k)]);
+  } else {
+    Ex[g.at(i, j, k)] = 0.0; Ex[g.at(i, j + 1, k)] = 0.0;
+    Ey[g.at(i, j, k)] = 0.0; Ey[g.at(i + 1, j, k)] = 0.0;
+    Ht[0] = 0.5 * (1 + A[0] + A[1]) * (Hx[g.at(i, j, k - 1)] + Hx[g.at(i + 1, j, k - 1)]);
+    Ht[1] = 0.5 * (1 + B[0] + B[1]) * (Hx[g.at(i, j, k)] + Hx[g.at(i + 1, j, k)]);
+    Ht[2] = 0.5 * (1 + A[2] + A[3]) * (Hy[g.at(i, j, k - 1)] + Hy[g.at(i, j + 1, k - 1)]);
+    Ht[3] = 0.5 * (1 + B[2] + B[3]) * (Hy[g.at(i, j, k)] + Hy[g.at(i, j + 1, k)]);
+  }
+  for (int a = 0; a < 4; a++) {
+    Hin[a] = 0.0;
+    for (int b = 0; b < 4; b++) Hin[a] = Hin[a] + (T)sf.A[a][b] * Ht[b];
+  }
+  double2 *z = zeta + zofs[s] + f * m.poles;
+  double *o = old + 16 * t;
+  for (int a = 0; a < 4; a++) {
+    Eout[a] = 0.0;
+    for (int b = 0; b < 4; b++) {
+      double xin = Hin[b];
+      double y = m.asymp[a][b] * xin;
+      int off = m.off[a][b];
+      double2 *zz = z + (off - m.off[0][0]);
+      double po = o[4 * a + b];
+      for (int r = 0; r < m.np[a][b]; r++) {
+        double2 a0 = q0[off + r], a1 = q1[off + r], a2 = q2[off + r], zv = zz[r];
+        double re = (a0.x * zv.x - a0.y * zv.y) + a1.x * po;
+        double im = (a0.x * zv.y + a0.y * zv.x) + a1.y * po;
+        re = re + a2.x * xin;
+        im = im + a2.y * xin;
+        zz[r] = make_double2(re, im);
+        y = y + re;
+      }
+      o[4 * a + b] = xin;
+      Eout[a] = Eout[a] + y;
+    }
+  }
+  T *et = etan + 4 * t;
+  for (int a = 0; a < 4; a++) {
+    T v = 0.0;
+    for (int b = 0; b < 4; b++) v = v + (T)sf.B[a][b] * Eout[b];
+    et[a] = v;
+  }
+}
+
+// One thread per corrected H value: apply its operations in order.
+struct SibcOp {
+  int64_t e1, e2;     // indices into etan
+  double c, d1, d2, n1, n2;
+  int kind, pad;
+};
+
+template <typename T>
+__global__ void k_sibc_h(Grid<T> g, const int64_t *tgt_index, const int *tgt_comp, const int64_t *tgt_start,
+                         int64_t ntgt, const SibcOp *ops, const T *etan)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntgt) return;
+  T *F = g.F[tgt_comp[t]];
+  const int64_t x = tgt_index[t];
+  T h = F[x];
+  for (int64_t q = tgt_start[t]; q < tgt_start[t + 1]; q++) {
+    const SibcOp o = ops[q];
+    if (o.kind == 0) { h = 0.0; continue; }
+    T c = (T)o.c, d1 = (T)o.d1;
+    T e1 = etan[o.e1];
+    if (o.kind == 1) {
+      h = h + c * (d1 * e1);
+    } else {
+      T e2 = etan[o.e2], d2 = (T)o.d2, n1 = (T)o.n1, n2 = (T)o.n2;
+      h = h + c * (n1 * (d1 * e1) + n2 * (d2 * e2));
+    }
+  }
+  F[x] = h;
+}
+
+// Finiteness scan of all field volumes.
+template <typename T>
+__global__ void k_finite(Grid<T> g, int64_t vol_padded, int *flag)
+{
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; t < vol_padded; t += stride)
+    for (int c = 0; c < 6; c++)
+      if (!isfinite((double)g.F[c][t])) { atomicExch(flag, 1); return; }
+}
+
+}  // namespace vgpu_dev

@@ -1,0 +1,174 @@
+"""Python front end of the drop-in solver path.
+
+Mirrors the reference's flow (src/vulture.c:77-197): read a mesh and set up
+(``Mesh``), advance the fields on the GPU (``GpuRun``), and write the same
+observer files (``Mesh.write_outputs``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from contextlib import contextmanager
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+
+@contextmanager
+def _chdir(path):
+    old = os.getcwd()
+    os.chdir(path)
+    try:
+        yield
+    finally:
+        os.chdir(old)
+
+
+class Mesh:
+    """A parsed and set-up mesh: the reference's state before propagate()."""
+
+    def __init__(self, path, log_path=None, verbose=False):
+        self.path = str(Path(path).resolve())
+        h = C.c_void_p()
+        N.check_host(N.lib().vhost_load(self.path.encode(), log_path.encode() if log_path else None, int(verbose),
+                                         C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            N.lib().vhost_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def problem(self, precision: str = "fp64") -> C.c_void_p:
+        p = C.c_void_p()
+        prec = N.VGPU_FP64 if precision == "fp64" else N.VGPU_FP32
+        N.check_host(N.lib().vhost_problem(self._h, prec, C.byref(p)))
+        return p
+
+    @property
+    def num_steps(self) -> int:
+        return int(N.lib().vhost_num_steps(self._h))
+
+    @property
+    def num_output_steps(self) -> int:
+        return int(N.lib().vhost_num_output_steps(self._h))
+
+    @property
+    def num_td(self) -> int:
+        return int(N.lib().vhost_num_td(self._h))
+
+    @property
+    def num_fd(self) -> int:
+        return int(N.lib().vhost_num_fd(self._h))
+
+    @property
+    def num_freq(self) -> int:
+        return int(N.lib().vhost_num_freq(self._h))
+
+    @property
+    def dt(self) -> float:
+        return float(N.lib().vhost_dt(self._h))
+
+    @property
+    def num_cells(self) -> int:
+        """Outer-box cells, the reference's spi/cell denominator."""
+        return int(N.lib().vhost_num_cells(self._h))
+
+    def observer_name(self, fd: bool, slot: int) -> str:
+        return N.lib().vhost_observer_name(self._h, int(fd), slot).decode()
+
+    def empty_outputs(self):
+        td = np.zeros((max(self.num_output_steps, 1), max(self.num_td, 1), 6))
+        re = np.zeros((max(self.num_fd, 1), 6, max(self.num_freq, 1)))
+        return td, re, np.zeros_like(re)
+
+    def write_outputs(self, directory, td, re, im, full_precision=False):
+        td = np.ascontiguousarray(td, dtype=np.float64)
+        re = np.ascontiguousarray(re, dtype=np.float64)
+        im = np.ascontiguousarray(im, dtype=np.float64)
+        Path(directory).mkdir(parents=True, exist_ok=True)
+        with _chdir(directory):
+            N.check_host(N.lib().vhost_write_outputs(self._h, td.ctypes.data, self.num_output_steps,
+                                                     re.ctypes.data, im.ctypes.data, int(full_precision)))
+
+
+class GpuRun:
+    """An engine instance on the current CUDA device (vgpu_create/run)."""
+
+    def __init__(self, mesh: Mesh, precision: str = "fp64"):
+        self.mesh = mesh
+        self.precision = precision
+        e = C.c_void_p()
+        N.check_gpu(N.lib().vgpu_create(mesh.problem(precision), C.byref(e)))
+        self._e = e
+
+    def run(self, nsteps=None):
+        n = self.mesh.num_steps - self.step if nsteps is None else nsteps
+        N.check_gpu(N.lib().vgpu_run(self._e, n))
+        return self
+
+    @property
+    def step(self) -> int:
+        return int(N.lib().vgpu_current_step(self._e))
+
+    def stats(self) -> N.VgpuStats:
+        st = N.VgpuStats()
+        N.check_gpu(N.lib().vgpu_get_stats(self._e, C.byref(st)))
+        return st
+
+    def td(self, steps=None):
+        m = self.mesh
+        steps = m.num_output_steps if steps is None else steps
+        out = np.zeros((max(steps, 1), max(m.num_td, 1), 6))
+        if m.num_td:
+            N.check_gpu(N.lib().vgpu_read_td(self._e, out.ctypes.data, steps))
+        return out
+
+    def dft(self):
+        m = self.mesh
+        re = np.zeros((max(m.num_fd, 1), 6, max(m.num_freq, 1)))
+        im = np.zeros_like(re)
+        if m.num_fd:
+            N.check_gpu(N.lib().vgpu_read_dft(self._e, re.ctypes.data, im.ctypes.data))
+        return re, im
+
+    def field(self, comp: int, shape):
+        out = np.zeros(shape)
+        N.check_gpu(N.lib().vgpu_read_field(self._e, comp, out.ctypes.data))
+        return out
+
+    def write_field(self, comp: int, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        N.check_gpu(N.lib().vgpu_write_field(self._e, comp, v.ctypes.data))
+
+    def check_finite(self):
+        N.check_gpu(N.lib().vgpu_check_finite(self._e))
+
+    def close(self):
+        if self._e:
+            N.lib().vgpu_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_mesh(mesh_path, out_dir, precision="fp64", full_precision=False):
+    """The reference's command-line flow on the GPU: set up, propagate, write outputs."""
+    m = Mesh(mesh_path)
+    g = GpuRun(m, precision).run()
+    re, im = g.dft()
+    m.write_outputs(out_dir, g.td(), re, im, full_precision)
+    g.close()
+    return m
