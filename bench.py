@@ -1,0 +1,319 @@
+"""Benchmark of the FDTD time-stepping path on B200.
+
+Workload (one GPU): the non-uniform mesh of 200x160x120 cells with seeded
+graded spacing (1-8 mm, neighbour ratio <= 1.3), 8-cell UPML on every face,
+one Debye block, a TFSF plane wave, 16 time-domain points and a 64x64 plane
+of frequency-domain observers over 200 frequencies; N_out = 216x176x136 =
+5,170,176 outer-box cells.  A step is one leapfrog time step of the whole
+grid (src/simulation.c:156-222).  The metric is Mcell-updates/s =
+N_out * steps / time (the reference's spi/cell denominator, src/timer.c:95).
+
+--gpus N runs N independent replicas, one per GPU (the path does not shard;
+per-GPU work is fixed, scaling "weak").  --impl reference times the
+reference's own CPU build on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+B_ALG = {"fp32": 4, "fp64": 8}        # bytes per word
+WORDS_E, WORDS_H = 15, 12             # algorithmic words per cell of the E and H sweeps
+WORKLOAD = dict(nt=4000, dims=(200, 160, 120), plane=64, nfreq=200, npml=8, ntd=16)
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def make_mesh(directory: Path, nt: int, plane: int = None) -> Path:
+    from vulture_b200 import meshgen
+
+    kw = dict(WORKLOAD)
+    kw["nt"] = nt
+    if plane is not None:
+        kw["plane"] = plane
+    return Path(meshgen.write(meshgen.config2(seed=2, **kw), directory / "config2.mesh"))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.out = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        if not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_record(kernel: str, precision: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(f"{kernel}:{precision}")
+
+
+def time_reference(binary: str, mesh_dir: Path, nt_lo: int, nt_hi: int, threads: int, plane=None):
+    """Per-step throughput of a reference build: two runs of the same mesh
+    with nt_lo and nt_hi steps; the difference removes set-up and output."""
+    from vulture_b200 import meshgen  # noqa: F401
+
+    walls = []
+    n_out = None
+    for nt in (nt_lo, nt_hi):
+        d = Path(tempfile.mkdtemp(prefix="vb_cpu_", dir=mesh_dir))
+        make_mesh(d, nt, plane)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        t0 = time.perf_counter()
+        r = subprocess.run([binary, "-n", str(threads), "config2.mesh"], cwd=d, env=env, capture_output=True,
+                           text=True)
+        walls.append(time.perf_counter() - t0)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed: {r.stderr[-400:]}")
+        if n_out is None:
+            import vulture_b200 as vb
+
+            n_out = vb.Mesh(d / "config2.mesh").num_cells
+        shutil.rmtree(d, ignore_errors=True)
+    dt = walls[1] - walls[0]
+    return n_out * (nt_hi - nt_lo) / dt / 1e6, walls
+
+
+def run_reference_arm(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    binary = ROOT / "oracle" / "_ref" / "vulture_ref_f32_omp"
+    base = {"metric": "Mcell-updates/s", "unit": "Mcell-updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "graded 200x160x120, UPML8, Debye, TFSF, 64x64x200 DFT plane + 16 TD",
+                       "n_out_cells": 5170176}}
+    if not binary.exists():
+        base["unavailable"] = "reference CPU build (oracle/_ref) not present"
+        print(json.dumps(base))
+        return
+    threads = os.cpu_count() or 1
+    # A bounded sample: the reference spends ~0.2 s per step in its serial
+    # point-DFT loop on this workload, so K timed steps are capped.
+    k = max(2, min(args.steps, 60))
+    w = max(1, min(args.warmup, 5))
+    work = Path(tempfile.mkdtemp(prefix="vb_refarm_"))
+    value, walls = time_reference(str(binary), work, w, w + k, threads)
+    shutil.rmtree(work, ignore_errors=True)
+    base.update({"value": value, "ms_per_step": 5170176 / (value * 1e6) * 1e3,
+                 "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+                                  "sample": f"config-2 mesh, vulture_ref_f32_omp -n {threads}, runs of {w} and "
+                                            f"{w + k} steps, difference of wall times {walls}"},
+                 "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(base))
+
+
+def run_gpu_arm(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import vulture_b200 as vb
+    from vulture_b200 import _native as N
+
+    prec = args.precision
+    work = Path(tempfile.mkdtemp(prefix=f"vb_bench_{rank}_"))
+    nt = max(WORKLOAD["nt"], args.warmup + args.steps)
+    mesh_path = make_mesh(work, nt)
+    old = os.getcwd()
+    os.chdir(work)
+    m = vb.Mesh(mesh_path.name)
+    os.chdir(old)
+    n_out = m.num_cells
+
+    # Device-resident timing: W untimed steps, then exactly K timed steps.
+    g = vb.GpuRun(m, prec)
+    g.run(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        g.run(args.steps)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    st = g.stats()
+    ms = st.run_ms
+    launches = int(st.kernel_launches)
+    g.check_finite()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_out * args.steps / (ms * 1e-3) / 1e6
+
+    # Roofline of the dominant kernel (bulk E sweep), timed live on the
+    # engine's stream with CUDA events.
+    kern = {}
+    for name, kid, words in (("bulk_e", N.VGPU_K_BULK_E, WORDS_E), ("bulk_h", N.VGPU_K_BULK_H, WORDS_H)):
+        kms, pts = g.time_kernel(kid, warmup=3, iters=20)
+        cells = pts / 3.0
+        kern[name] = dict(ms=kms, cells=cells, bytes=words * B_ALG[prec] * cells)
+    g.close()
+    peak, peak_kind = peaks()
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    achieved = kern[dom]["bytes"] / (kern[dom]["ms"] * 1e-3) / 1e9
+    tr = traffic_record(f"k_{dom}", prec)
+
+    # End to end through the C ABI: create (host->device upload of the
+    # problem), K steps, read the observers back (device->host).
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g2 = vb.GpuRun(m, prec)
+    g2.run(args.steps)
+    td = g2.td(args.steps)
+    re, im = g2.dft()
+    t1 = time.perf_counter()
+    e2e_wall = t1 - t0
+    dev_bytes = int(g2.stats().device_bytes)
+    g2.close()
+    e2e_value = world * n_out * args.steps / e2e_wall / 1e6
+    d2h = td.nbytes + re.nbytes + im.nbytes
+
+    # Plain FP64 on the same workload, for the FP32-vs-FP64 comparison.
+    fp64 = None
+    if prec == "fp32" and not args.no_fp64:
+        g3 = vb.GpuRun(m, "fp64")
+        g3.run(args.warmup)
+        g3.run(min(args.steps, 400))
+        st3 = g3.stats()
+        fp64 = n_out * st3.steps / (st3.run_ms * 1e-3) / 1e6
+        g3.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        binary = ROOT / "oracle" / "_ref" / "vulture_ref_f32_omp"
+        if binary.exists():
+            threads = os.cpu_count() or 1
+            cw = Path(tempfile.mkdtemp(prefix="vb_cpub_"))
+            try:
+                v, walls = time_reference(str(binary), cw, 5, 45, threads)
+                v2, walls2 = time_reference(str(binary), cw, 5, 45, threads, plane=0)
+                cpu = {"value": v, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+                       "sample": f"config-2 mesh on vulture_ref_f32_omp -n {threads}: runs of 5 and 45 steps, "
+                                 f"difference of wall times {[round(x, 2) for x in walls]} s",
+                       "without_fd_plane": v2}
+            except Exception as exc:  # the baseline is reported, never required
+                cpu = {"value": None, "error": str(exc)[:300]}
+            shutil.rmtree(cw, ignore_errors=True)
+
+    os.chdir(old)
+    shutil.rmtree(work, ignore_errors=True)
+    if rank == 0:
+        out = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": prec,
+            "data": "synthetic",
+            "config": {"workload": "graded 200x160x120, UPML8, Debye, TFSF, 64x64x200 DFT plane + 16 TD",
+                       "n_out_cells": n_out, "replicas": world, "l2": "inputs larger than L2 (~370 MB/GPU)",
+                       "precision": prec},
+            "roofline": {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": tr, "kernels": kern,
+                         "bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec]},
+            "e2e": {"value": e2e_value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": dev_bytes / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps, "wall_s": e2e_wall,
+                    "what": "vgpu_create (problem upload) + K steps + observer read-back"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "fp64_value": fp64,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -260,6 +260,17 @@ int vgpu_write_field(vgpu_engine *engine, int32_t component, const double *in);
 int vgpu_check_finite(vgpu_engine *engine);
 
 uint64_t vgpu_current_step(const vgpu_engine *engine);
+
+/* Kernels of one time step, for vgpu_time_kernel. */
+enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 };
+
+/* Profiling hook: launch one of the step's kernels `iters` times on the
+ * engine's stream (after `warmup` untimed launches) and report the mean
+ * device time per launch from CUDA events, plus the number of field points
+ * that kernel updates per launch.  It advances the fields it updates, so
+ * call it only when the run's results are no longer needed. */
+int vgpu_time_kernel(vgpu_engine *engine, int32_t kernel, int32_t warmup, int32_t iters, double *ms_per_launch,
+                     uint64_t *points);
 int vgpu_get_stats(const vgpu_engine *engine, vgpu_stats *stats);
 void vgpu_destroy(vgpu_engine *engine);
 

@@ -69,6 +69,8 @@ def lib() -> C.CDLL:
         "vgpu_write_field": (C.c_int, [P, C.c_int32, P]),
         "vgpu_check_finite": (C.c_int, [P]),
         "vgpu_current_step": (C.c_uint64, [P]),
+        "vgpu_time_kernel": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_uint64)]),
         "vgpu_get_stats": (C.c_int, [P, C.POINTER(VgpuStats)]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
@@ -96,4 +98,6 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vhost_num_fd", "vhost_num_freq", "vhost_dt", "vhost_num_cells", "vhost_write_outputs",
            "vhost_observer_name", "vhost_free", "vhost_last_error", "vhost_main", "vgpu_create", "vgpu_run",
            "vgpu_read_td", "vgpu_read_dft", "vgpu_read_field", "vgpu_write_field", "vgpu_check_finite",
-           "vgpu_current_step", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error"]
+           "vgpu_current_step", "vgpu_time_kernel", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error"]
+
+VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3

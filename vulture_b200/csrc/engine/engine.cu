@@ -70,6 +70,7 @@ struct EngineBase {
   virtual int read_field(int c, double *out) = 0;
   virtual int write_field(int c, const double *in) = 0;
   virtual int check_finite() = 0;
+  virtual int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) = 0;
   uint64_t step = 0;
   vgpu_stats stats{};
 };
@@ -769,6 +770,53 @@ struct Engine : EngineBase {
     return upload_volume(g.F[c], in);
   }
 
+  int launch_one(int kernel)
+  {
+    const dim3 blk(32, 8);
+    if (kernel == VGPU_K_BULK_E && !ube.empty()) {
+      dim3 grd((ube.nk() + 31) / 32, (ube.nj() + 7) / 8, ube.ni());
+      k_bulk_e<T><<<grd, blk, 0, s>>>(g, be[0], be[1], be[2], ube);
+    } else if (kernel == VGPU_K_BULK_H && !ubh.empty()) {
+      dim3 grd((ubh.nk() + 31) / 32, (ubh.nj() + 7) / 8, ubh.ni());
+      k_bulk_h<T><<<grd, blk, 0, s>>>(g, bh[0], bh[1], bh[2], ubh);
+    } else if (kernel == VGPU_K_PML_E && has_pml) {
+      k_pml_e<T><<<pml_grid, blk, 0, s>>>(g, pv);
+    } else if (kernel == VGPU_K_PML_H && has_pml) {
+      k_pml_h<T><<<pml_grid, blk, 0, s>>>(g, pv);
+    } else {
+      return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
+    }
+    return 0;
+  }
+
+  int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override
+  {
+    uint64_t pts = 0;
+    if (kernel == VGPU_K_BULK_E) for (int c = 0; c < 3; c++) pts += be[c].count();
+    else if (kernel == VGPU_K_BULK_H) for (int c = 0; c < 3; c++) pts += bh[c].count();
+    else if (kernel == VGPU_K_PML_E || kernel == VGPU_K_PML_H)
+      for (int r = 0; r < pv.nreg; r++)
+        for (int c = 0; c < 3; c++) pts += pv.lim[r][kernel == VGPU_K_PML_E ? c : 3 + c].count();
+    for (int q = 0; q < warmup; q++)
+      if (int rc = launch_one(kernel)) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    for (int q = 0; q < iters; q++)
+      if (int rc = launch_one(kernel)) return rc;
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaGetLastError());
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = iters > 0 ? t / iters : 0.0;
+    *points = pts;
+    return 0;
+  }
+
   int check_finite() override
   {
     int *flag;
@@ -799,11 +847,14 @@ static int validate(const vgpu_problem *p)
     if (!p->ide[a] || !p->idh[a]) return set_err(VGPU_EINVAL, "edge length arrays missing");
   // Every limit used by an update must keep its stencil inside the volume:
   // E updates read the -1 neighbours, H updates the +1 neighbours.
+  // Only the two axes other than the component's own are offset.
   auto in_grid = [&](const int32_t l[6], int field) {
     if (l[1] < l[0] || l[3] < l[2] || l[5] < l[4]) return true;
-    int lo = field <= 2 ? 1 : 0, hi_off = field <= 2 ? 1 : 2;
-    for (int a = 0; a < 3; a++)
+    for (int a = 0; a < 3; a++) {
+      bool reach = a != field % 3;
+      int lo = (field <= 2 && reach) ? 1 : 0, hi_off = (field > 2 && reach) ? 2 : 1;
       if (l[2 * a] < lo || l[2 * a + 1] > p->n[a] - hi_off) return false;
+    }
     return true;
   };
   for (int f = 0; f < 6; f++)
@@ -897,6 +948,13 @@ extern "C" int vgpu_check_finite(vgpu_engine *e)
 }
 
 extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
+
+extern "C" int vgpu_time_kernel(vgpu_engine *e, int32_t kernel, int32_t warmup, int32_t iters, double *ms,
+                                uint64_t *points)
+{
+  if (!e || !ms || !points || iters < 0 || warmup < 0) return set_err(VGPU_EINVAL, "invalid argument");
+  return e->impl->time_kernel(kernel, warmup, iters, ms, points);
+}
 
 extern "C" int vgpu_get_stats(const vgpu_engine *e, vgpu_stats *st)
 {

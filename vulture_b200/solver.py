@@ -149,6 +149,13 @@ class GpuRun:
         v = np.ascontiguousarray(values, dtype=np.float64)
         N.check_gpu(N.lib().vgpu_write_field(self._e, comp, v.ctypes.data))
 
+    def time_kernel(self, kernel: int, warmup=3, iters=20):
+        """Mean device ms per launch of one step kernel, and its field points."""
+        ms = C.c_double()
+        pts = C.c_uint64()
+        N.check_gpu(N.lib().vgpu_time_kernel(self._e, kernel, warmup, iters, C.byref(ms), C.byref(pts)))
+        return ms.value, pts.value
+
     def check_finite(self):
         N.check_gpu(N.lib().vgpu_check_finite(self._e))
 
