@@ -274,6 +274,28 @@ int vgpu_time_kernel(vgpu_engine *engine, int32_t kernel, int32_t warmup, int32_
 int vgpu_get_stats(const vgpu_engine *engine, vgpu_stats *stats);
 void vgpu_destroy(vgpu_engine *engine);
 
+/* Allocation-free running DFT.  No counterpart in the reference; it serves
+ * callers that cannot allocate device memory themselves (a host framework
+ * that owns every allocation, or code running where cudaMalloc is not
+ * allowed).  It adds num_rows rows of samples to running DFT sums:
+ *   re[s*num_freq + f] += x * cos(omega[f] * t_r)
+ *   im[s*num_freq + f] -= x * sin(omega[f] * t_r)
+ * for x = samples[r*num_series + s] and t_r = (first_step + r) * dt, in row
+ * order -- the observer DFT of src/observer.c:857-899.  All pointers are
+ * device pointers owned by the caller.  It calls no cudaMalloc or cudaFree:
+ * its twiddle table is a file-scope __device__ array of
+ * VGPU_STATIC_DFT_MAX_ENTRIES double2 (1 MiB), held on every GPU that loads
+ * the library until exit, and rows * freqs beyond that, or more than
+ * VGPU_STATIC_DFT_MAX_ROWS rows, are rejected with VGPU_EINVAL.  The first
+ * call on a device looks up the table's device address; make that call
+ * before any stream capture.  Calls share the one table, so calls that
+ * overlap on the GPU race; each call runs on the default stream and returns
+ * after it has finished. */
+#define VGPU_STATIC_DFT_MAX_ENTRIES 65536
+#define VGPU_STATIC_DFT_MAX_ROWS 256
+int vgpu_dft_accumulate_static(const double *samples, int32_t num_series, int32_t num_rows, const double *omega,
+                               int32_t num_freq, double dt, uint64_t first_step, double *re, double *im);
+
 /* Message of the last error on this thread. */
 const char *vgpu_last_error(void);
 

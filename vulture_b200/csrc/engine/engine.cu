@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.cuh"
 
@@ -960,6 +961,55 @@ extern "C" int vgpu_get_stats(const vgpu_engine *e, vgpu_stats *st)
 {
   if (!e || !st) return set_err(VGPU_EINVAL, "null argument");
   *st = e->impl->stats;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free running DFT for callers that cannot allocate device
+// memory.  The twiddle table lives in a file-scope device array; every GPU
+// that loads this library holds it (1 MiB) until the process exits.
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) double2 g_static_twiddle[VGPU_STATIC_DFT_MAX_ENTRIES];
+static std::mutex g_static_mu;
+static double2 *g_static_twiddle_ptr[64];  // device address of g_static_twiddle, per device
+
+extern "C" int vgpu_dft_accumulate_static(const double *samples, int32_t num_series, int32_t num_rows,
+                                          const double *omega, int32_t num_freq, double dt, uint64_t first_step,
+                                          double *re, double *im)
+{
+  if (!samples || !omega || !re || !im) return set_err(VGPU_EINVAL, "null device pointer");
+  if (num_series <= 0 || num_rows <= 0 || num_freq <= 0) return set_err(VGPU_EINVAL, "sizes must be positive");
+  if (num_rows > VGPU_STATIC_DFT_MAX_ROWS)
+    return set_err(VGPU_EINVAL, "num_rows %d exceeds the maximum of %d rows per call", num_rows, VGPU_STATIC_DFT_MAX_ROWS);
+  if ((int64_t)num_rows * num_freq > VGPU_STATIC_DFT_MAX_ENTRIES)
+    return set_err(VGPU_EINVAL, "num_rows * num_freq = %lld exceeds the static twiddle table of %d entries",
+                   (long long)num_rows * num_freq, VGPU_STATIC_DFT_MAX_ENTRIES);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_err(VGPU_EINVAL, "device ordinal %d out of range", dev);
+  double2 *tw = nullptr;
+  {
+    // First call on a device: look up the array's device address with that
+    // device current.  Host code may not use the symbol itself as a pointer.
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_twiddle_ptr[dev]) {
+      void *ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_twiddle);
+      if (e != cudaSuccess) return set_err(VGPU_ECUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      g_static_twiddle_ptr[dev] = (double2 *)ptr;
+    }
+    tw = g_static_twiddle_ptr[dev];
+  }
+  // The table is fully rewritten for the rows of this call before it is read,
+  // so nothing needs clearing; re/im carry the running sums between calls.
+  int64_t ntw = (int64_t)num_rows * num_freq;
+  k_twiddle<<<(unsigned)((ntw + 127) / 128), 128, 0, 0>>>(omega, num_freq, dt, first_step, 0, num_rows, tw);
+  dim3 blk(32, 8), grd((num_freq + 31) / 32, (num_series + 7) / 8);
+  k_dft_accumulate<<<grd, blk, sizeof(double) * 8 * num_rows, 0>>>(samples, num_series, num_freq, num_rows, 0,
+                                                                  num_rows, tw, re, im);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(0));
   return 0;
 }
 
