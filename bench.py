@@ -30,6 +30,9 @@ sys.path.insert(0, str(ROOT))
 
 B_ALG = {"fp32": 4, "fp64": 8}        # bytes per word
 WORDS_E, WORDS_H = 15, 12             # algorithmic words per cell of the E and H sweeps
+# The UPML sweeps also read and write their auxiliaries: PP and P per E
+# component (4 words), B per H component (2 words).
+WORDS_PML_E, WORDS_PML_H = WORDS_E + 12, WORDS_H + 6
 WORKLOAD = dict(nt=4000, dims=(200, 160, 120), plane=64, nfreq=200, npml=8, ntd=16)
 
 
@@ -213,18 +216,21 @@ def run_gpu_arm(args):
         ms = float(t.item())
     value = world * n_out * args.steps / (ms * 1e-3) / 1e6
 
-    # Roofline of the dominant kernel (bulk E sweep), timed live on the
-    # engine's stream with CUDA events.
+    # Roofline of the dominant kernel, each sweep timed live on the engine's
+    # stream with CUDA events.
     kern = {}
-    for name, kid, words in (("bulk_e", N.VGPU_K_BULK_E, WORDS_E), ("bulk_h", N.VGPU_K_BULK_H, WORDS_H)):
+    for name, kid, words in (("k_sweep_e_bulk", N.VGPU_K_BULK_E, WORDS_E), ("k_sweep_h_bulk", N.VGPU_K_BULK_H, WORDS_H),
+                             ("k_sweep_e_pml", N.VGPU_K_PML_E, WORDS_PML_E),
+                             ("k_sweep_h_pml", N.VGPU_K_PML_H, WORDS_PML_H)):
         kms, pts = g.time_kernel(kid, warmup=3, iters=20)
         cells = pts / 3.0
-        kern[name] = dict(ms=kms, cells=cells, bytes=words * B_ALG[prec] * cells)
+        kern[name] = dict(ms=kms, cells=cells, bytes=words * B_ALG[prec] * cells,
+                          gbs=words * B_ALG[prec] * cells / (kms * 1e-3) / 1e9)
     g.close()
     peak, peak_kind = peaks()
     dom = max(kern, key=lambda k: kern[k]["ms"])
     achieved = kern[dom]["bytes"] / (kern[dom]["ms"] * 1e-3) / 1e9
-    tr = traffic_record(f"k_{dom}", prec)
+    tr = traffic_record(dom, prec)
 
     # End to end through the C ABI: create (host->device upload of the
     # problem), K steps, read the observers back (device->host).
@@ -279,7 +285,7 @@ def run_gpu_arm(args):
             "config": {"workload": "graded 200x160x120, UPML8, Debye, TFSF, 64x64x200 DFT plane + 16 TD",
                        "n_out_cells": n_out, "replicas": world, "l2": "inputs larger than L2 (~370 MB/GPU)",
                        "precision": prec},
-            "roofline": {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": tr, "kernels": kern,
                          "bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec]},

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define VGPU_ABI_VERSION 1
+#define VGPU_ABI_VERSION 2
 
 /* Status codes. */
 #define VGPU_OK            0
@@ -220,6 +220,15 @@ typedef struct {
   const int32_t *fd_points;   /* [num_fd][3] */
   int32_t num_freq;
   const double *omega;        /* angular frequencies, num_freq */
+
+  /* Binary (TDOM_BINARY) observers (src/observer.c:1164-1198): every node of
+   * every binary observer, in the order the reference writes them to
+   * impulse.dat -- observers in mesh order, and within one observer k
+   * outermost, then j, then i, each advancing by the observer's step.
+   * Sampled with the point observers and delivered as float rows through a
+   * vgpu_bin_sink. */
+  int64_t num_bin;
+  const int32_t *bin_points;  /* [num_bin][3] grid indices */
 } vgpu_problem;
 
 typedef struct vgpu_engine vgpu_engine;
@@ -242,6 +251,22 @@ int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
  * continuing from the engine's current step.  Returns once the device has
  * finished. */
 int vgpu_run(vgpu_engine *engine, uint64_t nsteps);
+
+/* Receives binary-observer rows of consecutive output steps:
+ * rows[(r*num_points + q)*6 + c] is component c (Ex..Hz) of node q at output
+ * row first_row + r, rows counting from the window start out_start.  The
+ * values are float, as the reference writes them (src/observer.c:1168-1196).
+ * `rows` is valid only during the call.  Calls come from the thread running
+ * vgpu_run, in row order, while the device computes later steps; the last
+ * rows of a run arrive before vgpu_run returns. */
+typedef void (*vgpu_bin_sink)(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points,
+                              const float *rows);
+
+/* Install (or, with sink = NULL, remove) the binary-observer sink.  Replaces
+ * the per-step fwrite loop of updateImpulseDat (src/observer.c:1164-1198):
+ * the device gathers each step's nodes into a ring of 2 x 64 rows and copies
+ * every 64-step block to pinned host memory on a second stream. */
+int vgpu_set_bin_sink(vgpu_engine *engine, vgpu_bin_sink sink, void *user);
 
 /* Copy time-domain samples to the host: out[(s*num_td + p)*6 + c] for the
  * first `steps` steps of the output window. */

@@ -52,6 +52,27 @@ uint64_t vhost_num_cells(const vhost *h);
 int vhost_write_outputs(vhost *h, const double *td, uint64_t td_steps, const double *dft_re,
                         const double *dft_im, int32_t full_precision);
 
+/* Binary (TDOM_BINARY) observers (src/observer.c:1016-1212).  Nodes over
+ * all binary observers; 0 when there are none. */
+int64_t vhost_num_bin(const vhost *h);
+
+/* Write impulse.dat's header, excite.dat and process.dat into the current
+ * directory (initBinaryObservers, src/observer.c:1031-1151) and keep
+ * impulse.dat open for vhost_bin_sink.  A no-op without binary observers. */
+int vhost_bin_begin(vhost *h, int32_t full_precision);
+
+/* A vgpu_bin_sink (pass the vhost as `user`): appends the rows to impulse.dat
+ * in the reference's record layout (updateImpulseDat,
+ * src/observer.c:1164-1198). */
+void vhost_bin_sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows);
+
+/* Close impulse.dat; an error if any record failed to write. */
+int vhost_bin_end(vhost *h);
+
+/* xlines.dat, ylines.dat, zlines.dat: the mesh lines that the reference's
+ * grid set-up writes (src/grid.c:942-944). */
+int vhost_write_lines(vhost *h);
+
 /* Name of observer slot p of the time- (fd=0) or frequency-domain (fd=1) list. */
 const char *vhost_observer_name(const vhost *h, int32_t fd, int32_t p);
 

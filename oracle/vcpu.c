@@ -14,7 +14,7 @@
  *
  * Pinned against the reference itself: tests run the reference binaries
  * built by oracle/build_ref.sh on the same meshes and require identical
- * FP64 observer values (tests/test_oracle_pin.py).
+ * FP64 observer values (tests/test_oracle_reference.py).
  */
 #include <complex.h>
 #include <math.h>
@@ -65,6 +65,7 @@ typedef struct {
   real **Eyi, **Hzi, **PPyi, **Pyi, **Bzi;
   /* Outputs. */
   double *td;
+  float *bin;
   double *dre, *dim;
   uint64_t step;
 } vcpu;
@@ -157,6 +158,7 @@ void *API(create)(const vgpu_problem *p)
   if (p->num_steps > 0 && p->out_start < p->num_steps)
     nout = (p->out_stop < p->num_steps - 1 ? p->out_stop : p->num_steps - 1) - p->out_start + 1;
   s->td = calloc((size_t)(nout + 1) * (p->num_td + 1) * 6, sizeof(double));
+  s->bin = calloc((size_t)(nout + 1) * (p->num_bin + 1) * 6, sizeof(float));
   s->dre = calloc((size_t)(p->num_fd + 1) * 6 * (p->num_freq + 1), sizeof(double));
   s->dim = calloc((size_t)(p->num_fd + 1) * 6 * (p->num_freq + 1), sizeof(double));
   return s;
@@ -183,7 +185,7 @@ void API(destroy)(void *h)
   free(s->sz); free(s->sold); free(s->etan);
   for (int q = 0; q < p->num_planewaves; q++) { free(s->Eyi[q]); free(s->Hzi[q]); free(s->PPyi[q]); free(s->Pyi[q]); free(s->Bzi[q]); }
   free(s->Eyi); free(s->Hzi); free(s->PPyi); free(s->Pyi); free(s->Bzi);
-  free(s->td); free(s->dre); free(s->dim);
+  free(s->td); free(s->bin); free(s->dre); free(s->dim);
   free(s);
 }
 
@@ -199,6 +201,12 @@ static void update_observers(vcpu *s, uint64_t n)
     const int32_t *pt = &p->td_points[3 * q];
     int64_t x = IX(s, pt[0], pt[1], pt[2]);
     for (int c = 0; c < 6; c++) s->td[(row * p->num_td + q) * 6 + c] = (double)s->F[c][x];
+  }
+  /* Binary observers store float (src/observer.c:1168-1185). */
+  for (int64_t q = 0; q < p->num_bin; q++) {
+    const int32_t *pt = &p->bin_points[3 * q];
+    int64_t x = IX(s, pt[0], pt[1], pt[2]);
+    for (int c = 0; c < 6; c++) s->bin[(row * p->num_bin + q) * 6 + c] = (float)s->F[c][x];
   }
   for (int q = 0; q < p->num_fd; q++) {
     const int32_t *pt = &p->fd_points[3 * q];
@@ -870,6 +878,13 @@ int API(read_td)(void *h, double *out, uint64_t steps)
 {
   vcpu *s = h;
   memcpy(out, s->td, sizeof(double) * steps * s->p->num_td * 6);
+  return 0;
+}
+
+int API(read_bin)(void *h, float *out, uint64_t steps)
+{
+  vcpu *s = h;
+  memcpy(out, s->bin, sizeof(float) * steps * s->p->num_bin * 6);
   return 0;
 }
 

@@ -27,6 +27,7 @@ def _load():
         getattr(L, pre + "destroy").argtypes = [C.c_void_p]
         getattr(L, pre + "run").argtypes = [C.c_void_p, C.c_uint64]
         getattr(L, pre + "read_td").argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        getattr(L, pre + "read_bin").argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
         getattr(L, pre + "read_dft").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         getattr(L, pre + "read_field").argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         getattr(L, pre + "write_field").argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
@@ -59,6 +60,15 @@ class CpuRun:
         out = np.zeros((max(steps, 1), max(m.num_td, 1), 6))
         if m.num_td:
             self._f("read_td")(self._h, out.ctypes.data, steps)
+        return out
+
+    def bin(self, steps=None):
+        """Binary-observer rows [steps][num_bin][6] as float32."""
+        m = self.mesh
+        steps = m.num_output_steps if steps is None else steps
+        out = np.zeros((steps, m.num_bin, 6), dtype=np.float32)
+        if m.num_bin and steps:
+            self._f("read_bin")(self._h, out.ctypes.data, steps)
         return out
 
     def dft(self):

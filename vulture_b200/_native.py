@@ -29,6 +29,10 @@ class VgpuStats(C.Structure):
                 ("device_bytes", C.c_uint64)]
 
 
+# void sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows)
+BIN_SINK = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_uint32, C.c_int64, C.POINTER(C.c_float))
+
+
 class NativeError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[{code}] {msg}")
@@ -58,6 +62,11 @@ def lib() -> C.CDLL:
         "vhost_num_cells": (C.c_uint64, [P]),
         "vhost_write_outputs": (C.c_int, [P, P, C.c_uint64, P, P, C.c_int32]),
         "vhost_observer_name": (C.c_char_p, [P, C.c_int32, C.c_int32]),
+        "vhost_num_bin": (C.c_int64, [P]),
+        "vhost_bin_begin": (C.c_int, [P, C.c_int32]),
+        "vhost_bin_sink": (None, [P, C.c_uint64, C.c_uint32, C.c_int64, P]),
+        "vhost_bin_end": (C.c_int, [P]),
+        "vhost_write_lines": (C.c_int, [P]),
         "vhost_free": (None, [P]),
         "vhost_last_error": (C.c_char_p, []),
         "vhost_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),
@@ -72,6 +81,7 @@ def lib() -> C.CDLL:
         "vgpu_time_kernel": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                        C.POINTER(C.c_uint64)]),
         "vgpu_get_stats": (C.c_int, [P, C.POINTER(VgpuStats)]),
+        "vgpu_set_bin_sink": (C.c_int, [P, P, P]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
     }
@@ -98,6 +108,8 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vhost_num_fd", "vhost_num_freq", "vhost_dt", "vhost_num_cells", "vhost_write_outputs",
            "vhost_observer_name", "vhost_free", "vhost_last_error", "vhost_main", "vgpu_create", "vgpu_run",
            "vgpu_read_td", "vgpu_read_dft", "vgpu_read_field", "vgpu_write_field", "vgpu_check_finite",
-           "vgpu_current_step", "vgpu_time_kernel", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error"]
+           "vgpu_current_step", "vgpu_time_kernel", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error",
+           "vgpu_set_bin_sink", "vgpu_dft_accumulate_static", "vhost_num_bin", "vhost_bin_begin", "vhost_bin_sink",
+           "vhost_bin_end", "vhost_write_lines"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <map>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -72,6 +73,8 @@ struct EngineBase {
   virtual int write_field(int c, const double *in) = 0;
   virtual int check_finite() = 0;
   virtual int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) = 0;
+  vgpu_bin_sink bin_sink = nullptr;
+  void *bin_user = nullptr;
   uint64_t step = 0;
   vgpu_stats stats{};
 };
@@ -105,7 +108,6 @@ struct Engine : EngineBase {
   // PML
   bool has_pml = false;
   PmlView<T> pv{};
-  dim3 pml_grid;
   // Mur
   MurView mve{}, mvh{};
   int64_t mur_total_e = 0, mur_total_h = 0;
@@ -142,6 +144,21 @@ struct Engine : EngineBase {
   double *d_stage = nullptr, *d_re = nullptr, *d_im = nullptr, *d_omega = nullptr;
   double2 *d_tw = nullptr;
   uint64_t nout = 0;
+  // binary observers: device ring of 2 blocks x kChunk rows, pinned host copy
+  int *d_bin_pts = nullptr;
+  float *d_bin = nullptr, *h_bin = nullptr;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_fill[2] = {}, ev_copy[2] = {};
+  struct BinBlock {
+    bool pending;
+    uint64_t row0;
+    uint32_t nrows;
+  } bin_blk[2] = {};
+  // fused sweeps
+  CoefIndex cie{}, cih{};
+  // Tile lists: bulk tiles first, then the PML regions' tiles.
+  Tile *d_tiles_e = nullptr, *d_tiles_h = nullptr;
+  int nbulk_e = 0, nbulk_h = 0, npml_e = 0, npml_h = 0;
   // graph
   cudaGraphExec_t graph = nullptr;
   uint64_t launches_per_step = 0;
@@ -149,7 +166,15 @@ struct Engine : EngineBase {
   ~Engine() override
   {
     if (graph) cudaGraphExecDestroy(graph);
+    if (s) cudaStreamSynchronize(s);
+    if (cs) cudaStreamSynchronize(cs);
     mem.free_all();
+    if (h_bin) cudaFreeHost(h_bin);
+    for (int q = 0; q < 2; q++) {
+      if (ev_fill[q]) cudaEventDestroy(ev_fill[q]);
+      if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
+    }
+    if (cs) cudaStreamDestroy(cs);
     if (s) cudaStreamDestroy(s);
   }
 
@@ -161,12 +186,14 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  int upload_real(T **d, const double *h, size_t n)
+  // Copies n values into a device array of n + pad elements (zero tail), so
+  // lanes of a tile that run into the row padding read valid memory.
+  int upload_real(T **d, const double *h, size_t n, size_t pad = 0)
   {
-    std::vector<T> tmp(n ? n : 1);
+    std::vector<T> tmp(n + pad ? n + pad : 1, (T)0);
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
-    if (mem.alloc(d, n)) return VGPU_ENOMEM;
-    if (n) CK(cudaMemcpy(*d, tmp.data(), sizeof(T) * n, cudaMemcpyHostToDevice));
+    if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
+    if (n + pad) CK(cudaMemcpy(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice));
     return 0;
   }
 
@@ -206,9 +233,9 @@ struct Engine : EngineBase {
     }
     for (int a = 0; a < 3; a++) {
       T *d;
-      if (int rc = upload_real(&d, p.ide[a], p.n[a])) return rc;
+      if (int rc = upload_real(&d, p.ide[a], p.n[a], 64)) return rc;
       g.ide[a] = d;
-      if (int rc = upload_real(&d, p.idh[a], p.n[a])) return rc;
+      if (int rc = upload_real(&d, p.idh[a], p.n[a], 64)) return rc;
       g.idh[a] = d;
     }
     if (mem.alloc(&d_step, 1)) return VGPU_ENOMEM;
@@ -230,6 +257,8 @@ struct Engine : EngineBase {
     if (int rc = setup_planewaves()) return rc;
     setup_ghost();
     if (int rc = setup_observers()) return rc;
+    if (int rc = setup_tiles()) return rc;
+    if (int rc = setup_coef_index()) return rc;
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
     stats.device_bytes = mem.bytes;
@@ -251,22 +280,12 @@ struct Engine : EngineBase {
   int setup_pml()
   {
     pv.nreg = 0;
-    int plane = 0, maxj = 1, maxk = 1;
     for (int r = 0; r < 6; r++) {
       if (!p.pml_present[r]) continue;
       int q = pv.nreg++;
       Box bb[6];
       for (int f = 0; f < 6; f++) bb[f] = box_from(p.pml_flim[r][f]);
       for (int f = 0; f < 6; f++) pv.lim[q][f] = bb[f];
-      Box all[6] = { bb[0], bb[1], bb[2], bb[3], bb[4], bb[5] };
-      Box ue = unite(all), uh = unite(all + 3);
-      Box u{ std::min(ue.i0, uh.i0), std::max(ue.i1, uh.i1), std::min(ue.j0, uh.j0), std::max(ue.j1, uh.j1),
-             std::min(ue.k0, uh.k0), std::max(ue.k1, uh.k1) };
-      pv.uni[q] = u;
-      pv.reg_plane0[q] = plane;
-      plane += u.ni();
-      maxj = std::max(maxj, u.nj());
-      maxk = std::max(maxk, u.nk());
       for (int c = 0; c < 3; c++) {
         int64_t ne = bb[c].count(), nh = bb[3 + c].count();
         if (mem.alloc(&pv.PP[q][c], ne) || mem.alloc(&pv.P[q][c], ne) || mem.alloc(&pv.B[q][c], nh)) return VGPU_ENOMEM;
@@ -275,19 +294,17 @@ struct Engine : EngineBase {
         CK(cudaMemset(pv.B[q][c], 0, sizeof(T) * (nh ? nh : 1)));
       }
     }
-    pv.reg_plane0[pv.nreg] = plane;
     has_pml = pv.nreg > 0;
     if (!has_pml) return 0;
     for (int a = 0; a < 3; a++) {
       T *d;
-      if (int rc = upload_real(&d, p.pml_ad[a], p.n[a])) return rc; pv.ad[a] = d;
-      if (int rc = upload_real(&d, p.pml_bd[a], p.n[a])) return rc; pv.bd[a] = d;
-      if (int rc = upload_real(&d, p.pml_ah[a], p.n[a])) return rc; pv.ah[a] = d;
-      if (int rc = upload_real(&d, p.pml_bh[a], p.n[a])) return rc; pv.bh[a] = d;
-      if (int rc = upload_real(&d, p.pml_ibd[a], p.n[a])) return rc; pv.ibd[a] = d;
-      if (int rc = upload_real(&d, p.pml_ibh[a], p.n[a])) return rc; pv.ibh[a] = d;
+      if (int rc = upload_real(&d, p.pml_ad[a], p.n[a], 64)) return rc; pv.ad[a] = d;
+      if (int rc = upload_real(&d, p.pml_bd[a], p.n[a], 64)) return rc; pv.bd[a] = d;
+      if (int rc = upload_real(&d, p.pml_ah[a], p.n[a], 64)) return rc; pv.ah[a] = d;
+      if (int rc = upload_real(&d, p.pml_bh[a], p.n[a], 64)) return rc; pv.bh[a] = d;
+      if (int rc = upload_real(&d, p.pml_ibd[a], p.n[a], 64)) return rc; pv.ibd[a] = d;
+      if (int rc = upload_real(&d, p.pml_ibh[a], p.n[a], 64)) return rc; pv.ibh[a] = d;
     }
-    pml_grid = dim3((maxk + 31) / 32, (maxj + 7) / 8, plane);
     return 0;
   }
 
@@ -553,6 +570,93 @@ struct Engine : EngineBase {
     return 0;
   }
 
+  static void add_tiles(std::vector<Tile> &out, int region, const Box &u, int ti)
+  {
+    if (u.empty()) return;
+    int kstart = (u.k0 / 32) * 32;
+    for (int i = u.i0; i <= u.i1; i += ti)
+      for (int j = u.j0; j <= u.j1; j += 8)
+        for (int k = kstart; k <= u.k1; k += 32) out.push_back(Tile{ region, i, std::min(i + ti - 1, u.i1), j, k, 0 });
+  }
+
+  // Tile lists of the fused E and H sweeps: the bulk union box and each PML
+  // region's union box, i runs sized so the grid fills the GPU a few times.
+  int setup_tiles()
+  {
+    int64_t cells = (int64_t)ube.count();
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    int64_t target_tiles = (int64_t)nsm * 8 * 4;
+    int ti = (int)std::max<int64_t>(1, std::min<int64_t>(16, cells / (256 * target_tiles)));
+    std::vector<Tile> te, th;
+    add_tiles(te, -1, ube, ti);
+    add_tiles(th, -1, ubh, ti);
+    nbulk_e = (int)te.size();
+    nbulk_h = (int)th.size();
+    for (int r = 0; r < pv.nreg; r++) {
+      Box e3[3] = { pv.lim[r][0], pv.lim[r][1], pv.lim[r][2] };
+      Box h3[3] = { pv.lim[r][3], pv.lim[r][4], pv.lim[r][5] };
+      add_tiles(te, r, unite(e3), ti);
+      add_tiles(th, r, unite(h3), ti);
+    }
+    npml_e = (int)te.size() - nbulk_e;
+    npml_h = (int)th.size() - nbulk_h;
+    if (upload(&d_tiles_e, te.data(), te.size()) || upload(&d_tiles_h, th.data(), th.size())) return VGPU_ENOMEM;
+    return 0;
+  }
+
+  // Distinct coefficient tuples per cell: (alpha, beta) x 3 for E and
+  // gamma x 3 for H.  Up to 256 tuples compress to one byte per cell.
+  int build_index(int first, int count, CoefIndex &out)
+  {
+    out = CoefIndex{};
+    std::vector<T> table;
+    std::vector<uint8_t> idx((size_t)vol, 0);
+    struct Key {
+      T v[6];
+      bool operator<(const Key &o) const { return memcmp(v, o.v, sizeof v) < 0; }
+    };
+    std::map<Key, int> seen;
+    int last = -1;
+    Key lastk{};
+    for (int i = 0; i < p.n[0]; i++)
+      for (int j = 0; j < p.n[1]; j++)
+        for (int k = 0; k < p.n[2]; k++) {
+          int64_t hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
+          Key key{};
+          for (int c = 0; c < count; c++) key.v[c] = (T)p.coef[first + c][hq];
+          int q = -1;
+          if (last >= 0 && memcmp(key.v, lastk.v, sizeof key.v) == 0) q = last;
+          if (q < 0) {
+            auto it = seen.find(key);
+            if (it != seen.end()) q = it->second;
+          }
+          if (q < 0) {
+            if (seen.size() == 256) return 0;  // too many: keep the full volumes
+            q = (int)seen.size();
+            seen.emplace(key, q);
+            for (int c = 0; c < count; c++) table.push_back(key.v[c]);
+          }
+          last = q;
+          lastk = key;
+          idx[(int64_t)i * g.s0 + (int64_t)j * g.s1 + k] = (uint8_t)q;
+        }
+    uint8_t *d_idx;
+    T *d_tab;
+    if (upload(&d_idx, idx.data(), idx.size()) || upload(&d_tab, table.data(), table.size())) return VGPU_ENOMEM;
+    out.idx = d_idx;
+    out.table = d_tab;
+    out.ntab = (int)seen.size();
+    return 0;
+  }
+
+  int setup_coef_index()
+  {
+    if (getenv("VGPU_FULL_COEFFICIENTS")) return 0;
+    if (int rc = build_index(0, 6, cie)) return rc;
+    return build_index(6, 3, cih);
+  }
+
   void setup_ghost()
   {
     int maxp = 1;
@@ -586,6 +690,54 @@ struct Engine : EngineBase {
     CK(cudaMemset(d_re, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
     CK(cudaMemset(d_im, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
     if (upload(&d_omega, p.omega, p.num_freq)) return VGPU_ENOMEM;
+    return setup_bin();
+  }
+
+  int setup_bin()
+  {
+    if (p.num_bin <= 0) return 0;
+    if (!p.bin_points) return set_err(VGPU_EINVAL, "num_bin > 0 with no bin_points");
+    for (int64_t q = 0; q < p.num_bin; q++)
+      for (int a = 0; a < 3; a++) {
+        int v = p.bin_points[3 * q + a];
+        if (v < 0 || v >= p.n[a]) return set_err(VGPU_EINVAL, "binary observer node %lld outside the grid", (long long)q);
+      }
+    size_t row = (size_t)p.num_bin * 6;
+    if (upload(&d_bin_pts, p.bin_points, (size_t)p.num_bin * 3) || mem.alloc(&d_bin, 2 * kChunk * row))
+      return VGPU_ENOMEM;
+    CK(cudaMallocHost(&h_bin, sizeof(float) * 2 * kChunk * row));
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    for (int q = 0; q < 2; q++) {
+      CK(cudaEventCreateWithFlags(&ev_fill[q], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&ev_copy[q], cudaEventDisableTiming));
+    }
+    return 0;
+  }
+
+  // Hand the rows of ring block q to the sink once their copy has landed.
+  int bin_deliver(int q)
+  {
+    BinBlock &b = bin_blk[q];
+    if (!b.pending) return 0;
+    b.pending = false;
+    CK(cudaEventSynchronize(ev_copy[q]));
+    size_t row = (size_t)p.num_bin * 6;
+    const float *rows = h_bin + ((size_t)q * kChunk + (b.row0 + p.out_start) % kChunk) * row;
+    if (bin_sink) bin_sink(bin_user, b.row0, b.nrows, p.num_bin, rows);
+    return 0;
+  }
+
+  // Copy output steps lo..hi (absolute, inside one aligned chunk) of ring
+  // block q to pinned host memory on the copy stream.
+  int bin_enqueue(int q, uint64_t lo, uint64_t hi)
+  {
+    size_t row = (size_t)p.num_bin * 6;
+    size_t off = ((size_t)q * kChunk + lo % kChunk) * row;
+    CK(cudaEventRecord(ev_fill[q], s));
+    CK(cudaStreamWaitEvent(cs, ev_fill[q], 0));
+    CK(cudaMemcpyAsync(h_bin + off, d_bin + off, sizeof(float) * (hi - lo + 1) * row, cudaMemcpyDeviceToHost, cs));
+    CK(cudaEventRecord(ev_copy[q], cs));
+    bin_blk[q] = BinBlock{ true, lo - p.out_start, (uint32_t)(hi - lo + 1) };
     return 0;
   }
 
@@ -602,13 +754,16 @@ struct Engine : EngineBase {
                                                         0, p.out_start, p.out_stop, kTB);
       launches++;
     }
-    if (has_pml) { k_pml_e<T><<<pml_grid, blk, 0, s>>>(g, pv); launches++; }
-    if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
-    if (!ube.empty()) {
-      dim3 grd((ube.nk() + 31) / 32, (ube.nj() + 7) / 8, ube.ni());
-      k_bulk_e<T><<<grd, blk, 0, s>>>(g, be[0], be[1], be[2], ube);
+    if (p.num_bin > 0) {
+      k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step,
+                                                                      p.out_start, p.out_stop, kChunk);
       launches++;
     }
+    // Mur reads the neighbours' pre-update E, so it precedes the sweeps; the
+    // PML and bulk sweeps touch disjoint E points.
+    if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
+    if (int rc = launch_one(VGPU_K_PML_E, false, &launches)) return rc;
+    if (int rc = launch_one(VGPU_K_BULK_E, false, &launches)) return rc;
     if (n_debye) {
       k_debye<T><<<blocks_for(debye_total, 128), 128, 0, s>>>(g, d_debye, n_debye, debye_total, d_J, d_lastE, d_dcoef);
       launches++;
@@ -634,13 +789,9 @@ struct Engine : EngineBase {
       k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 6), 128, 0, s>>>(g, gv, 1, 0);
       launches++;
     }
-    if (has_pml) { k_pml_h<T><<<pml_grid, blk, 0, s>>>(g, pv); launches++; }
     if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
-    if (!ubh.empty()) {
-      dim3 grd((ubh.nk() + 31) / 32, (ubh.nj() + 7) / 8, ubh.ni());
-      k_bulk_h<T><<<grd, blk, 0, s>>>(g, bh[0], bh[1], bh[2], ubh);
-      launches++;
-    }
+    if (int rc = launch_one(VGPU_K_PML_H, false, &launches)) return rc;
+    if (int rc = launch_one(VGPU_K_BULK_H, false, &launches)) return rc;
     if (nsibc && ntgt) {
       k_sibc_h<T><<<blocks_for(ntgt, 128), 128, 0, s>>>(g, d_tgt_index, d_tgt_comp, d_tgt_start, ntgt, d_ops, d_etan);
       launches++;
@@ -709,6 +860,12 @@ struct Engine : EngineBase {
       // Chunks stay aligned so the DFT staging rows of one chunk never wrap.
       uint64_t room = kChunk - (n0 % kChunk);
       uint64_t m = std::min<uint64_t>(room, nsteps - done);
+      const int q = (int)((n0 / kChunk) & 1);
+      // The ring block this chunk fills last held the chunk two back: hand
+      // those rows over (the device is busy with the previous chunk) before
+      // they are overwritten.
+      if (p.num_bin > 0)
+        if (int rc = bin_deliver(q)) return rc;
       if (m == (uint64_t)kChunk) {
         CK(cudaGraphLaunch(graph, s));
       } else {
@@ -719,12 +876,22 @@ struct Engine : EngineBase {
       done += m;
       // Output rows produced in this chunk.
       uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
+      if (p.num_bin > 0 && bin_sink && hi >= lo && lo <= p.out_stop) {
+        if (int rc = bin_enqueue(q, lo, hi)) return rc;
+      }
       if (p.num_fd && hi >= lo) {
         if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
       }
     }
     CK(cudaEventRecord(e1, s));
     CK(cudaEventSynchronize(e1));
+    if (p.num_bin > 0) {
+      // The older pending block first.
+      int a = 0, b = 1;
+      if (bin_blk[1].pending && (!bin_blk[0].pending || bin_blk[1].row0 < bin_blk[0].row0)) a = 1, b = 0;
+      if (int rc = bin_deliver(a)) return rc;
+      if (int rc = bin_deliver(b)) return rc;
+    }
     CK(cudaGetLastError());
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
@@ -771,30 +938,33 @@ struct Engine : EngineBase {
     return upload_volume(g.F[c], in);
   }
 
-  int launch_one(int kernel)
+  // Launch one sweep over its tile list; with `required` an empty list is an
+  // error (profiling), otherwise it launches nothing.
+  int launch_one(int kernel, bool required = true, uint64_t *count = nullptr)
   {
     const dim3 blk(32, 8);
-    if (kernel == VGPU_K_BULK_E && !ube.empty()) {
-      dim3 grd((ube.nk() + 31) / 32, (ube.nj() + 7) / 8, ube.ni());
-      k_bulk_e<T><<<grd, blk, 0, s>>>(g, be[0], be[1], be[2], ube);
-    } else if (kernel == VGPU_K_BULK_H && !ubh.empty()) {
-      dim3 grd((ubh.nk() + 31) / 32, (ubh.nj() + 7) / 8, ubh.ni());
-      k_bulk_h<T><<<grd, blk, 0, s>>>(g, bh[0], bh[1], bh[2], ubh);
-    } else if (kernel == VGPU_K_PML_E && has_pml) {
-      k_pml_e<T><<<pml_grid, blk, 0, s>>>(g, pv);
-    } else if (kernel == VGPU_K_PML_H && has_pml) {
-      k_pml_h<T><<<pml_grid, blk, 0, s>>>(g, pv);
+    if (kernel == VGPU_K_BULK_E && nbulk_e) {
+      k_sweep_e<T, false><<<nbulk_e, blk, 0, s>>>(g, d_tiles_e, be[0], be[1], be[2], pv, cie);
+    } else if (kernel == VGPU_K_BULK_H && nbulk_h) {
+      k_sweep_h<T, false><<<nbulk_h, blk, 0, s>>>(g, d_tiles_h, bh[0], bh[1], bh[2], pv, cih);
+    } else if (kernel == VGPU_K_PML_E && npml_e) {
+      k_sweep_e<T, true><<<npml_e, blk, 0, s>>>(g, d_tiles_e + nbulk_e, be[0], be[1], be[2], pv, cie);
+    } else if (kernel == VGPU_K_PML_H && npml_h) {
+      k_sweep_h<T, true><<<npml_h, blk, 0, s>>>(g, d_tiles_h + nbulk_h, bh[0], bh[1], bh[2], pv, cih);
     } else {
+      if (!required) return 0;
       return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
     }
+    if (count) ++*count;
     return 0;
   }
 
   int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override
   {
     uint64_t pts = 0;
-    if (kernel == VGPU_K_BULK_E) for (int c = 0; c < 3; c++) pts += be[c].count();
-    else if (kernel == VGPU_K_BULK_H) for (int c = 0; c < 3; c++) pts += bh[c].count();
+    if (kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) {
+      for (int c = 0; c < 3; c++) pts += (kernel == VGPU_K_BULK_H ? bh : be)[c].count();
+    }
     else if (kernel == VGPU_K_PML_E || kernel == VGPU_K_PML_H)
       for (int r = 0; r < pv.nreg; r++)
         for (int c = 0; c < 3; c++) pts += pv.lim[r][kernel == VGPU_K_PML_E ? c : 3 + c].count();
@@ -949,6 +1119,14 @@ extern "C" int vgpu_check_finite(vgpu_engine *e)
 }
 
 extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
+
+extern "C" int vgpu_set_bin_sink(vgpu_engine *e, vgpu_bin_sink sink, void *user)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  e->impl->bin_sink = sink;
+  e->impl->bin_user = user;
+  return 0;
+}
 
 extern "C" int vgpu_time_kernel(vgpu_engine *e, int32_t kernel, int32_t warmup, int32_t iters, double *ms,
                                 uint64_t *points)

@@ -228,6 +228,10 @@ struct vhost {
   double *omega;
   int num_td, num_fd;
   int32_t *td_points, *fd_points;
+  int64_t num_bin;            /* nodes of all TDOM_BINARY observers */
+  int32_t *bin_points;
+  FILE *impulse;              /* impulse.dat while binary rows stream in */
+  int impulse_failed;
 
   /* Assembled problem (owned). */
   vgpu_problem prob;

@@ -83,6 +83,13 @@ int vhost_main(int argc, char **argv)
     vhost_free(h);
     return 6;
   }
+  /* Files the reference's set-up writes: mesh lines (initGrid) and the
+   * binary observers' headers (initObservers). */
+  if (vhost_write_lines(h) || vhost_bin_begin(h, full)) {
+    fprintf(stderr, "Vulture: *** Error: %s\n", vhost_last_error());
+    vhost_free(h);
+    return 6;
+  }
   uint64_t nout = vhost_num_output_steps(h);
   double *td = calloc((size_t)(nout ? nout : 1) * (p->num_td ? p->num_td : 1) * 6, sizeof(double));
   size_t ndft = (size_t)(p->num_fd ? p->num_fd : 1) * 6 * (p->num_freq ? p->num_freq : 1);
@@ -91,13 +98,14 @@ int vhost_main(int argc, char **argv)
   if (!preprocess && p->num_steps > 0) {
     vgpu_engine *e = NULL;
     rc = vgpu_create(p, &e);
+    if (!rc && p->num_bin) rc = vgpu_set_bin_sink(e, vhost_bin_sink, h);
     if (!rc) rc = vgpu_run(e, p->num_steps);
     if (!rc && p->num_td) rc = vgpu_read_td(e, td, nout);
     if (!rc && p->num_fd) rc = vgpu_read_dft(e, re, im);
     if (rc) fprintf(stderr, "Vulture: *** Error: %s\n", vgpu_last_error());
     vgpu_destroy(e);
   }
-  if (!rc && vhost_write_outputs(h, td, preprocess ? 0 : nout, re, im, full)) {
+  if (!rc && (vhost_bin_end(h) || vhost_write_outputs(h, td, preprocess ? 0 : nout, re, im, full))) {
     fprintf(stderr, "Vulture: *** Error: %s\n", vhost_last_error());
     rc = -1;
   }

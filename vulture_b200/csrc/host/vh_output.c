@@ -119,3 +119,137 @@ int vhost_write_outputs(vhost *h, const double *td, uint64_t td_steps, const dou
   }
   return 0;
 }
+
+/* ---- binary observers (src/observer.c:1016-1212) ---- */
+
+int64_t vhost_num_bin(const vhost *h);
+
+/* Mesh lines, as initGrid() leaves them in the working directory
+ * (src/grid.c:942-944, 1164-1178). */
+int vhost_write_lines(vhost *h)
+{
+  if (!h) { vh_set_tls_error("null host handle"); return VGPU_EINVAL; }
+  static const char *names[3] = { "xlines.dat", "ylines.dat", "zlines.dat" };
+  for (int a = 0; a < 3; a++) {
+    FILE *fp = fopen(names[a], "w");
+    if (!fp) {
+      vh_fail(h, "*** Error: Failed to open %s file.", names[a]);
+      vh_set_tls_error(h->err);
+      return VGPU_EINVAL;
+    }
+    for (int i = 0; i < h->num_lines[a]; i++) fprintf(fp, "%d %e\n", i, h->lines[a][i]);
+    fclose(fp);
+  }
+  return 0;
+}
+
+static int bin_fail(vhost *h, const char *what)
+{
+  vh_fail(h, "*** Error: Failed to open %s file", what);
+  vh_set_tls_error(h->err);
+  return VGPU_EINVAL;
+}
+
+/* impulse.dat header, excite.dat and process.dat (src/observer.c:1031-1162). */
+int vhost_bin_begin(vhost *h, int32_t full_precision)
+{
+  if (!h) { vh_set_tls_error("null host handle"); return VGPU_EINVAL; }
+  int nbin_obs = 0;
+  vh_observer *first = NULL;
+  for (int o = 0; o < h->num_obs; o++)
+    if (h->obs[o].kind == OBS_TD_BINARY) {
+      if (!first) first = &h->obs[o];
+      nbin_obs++;
+    }
+  if (!nbin_obs) return 0;
+  if (h->impulse) fclose(h->impulse);
+  h->impulse_failed = 0;
+
+  /* impulse.dat: the output step count as a 4-byte int and dt as a float.
+   * The reference writes sizeof(float) bytes of its `real` dt; with
+   * real=float (the shipped build) that is the float written here. */
+  h->impulse = fopen("impulse.dat", "wb");
+  if (!h->impulse) return bin_fail(h, "impulse.dat");
+  int32_t nout = (int32_t)(uint32_t)(h->out_stop - h->out_start + 1UL);
+  float dtf = (float)h->dt;
+  if (fwrite(&nout, sizeof nout, 1, h->impulse) != 1 || fwrite(&dtf, sizeof dtf, 1, h->impulse) != 1)
+    h->impulse_failed = 1;
+
+  /* excite.dat: waveform 0 at every step's E time. */
+  FILE *fp = fopen("excite.dat", "w");
+  if (!fp) return bin_fail(h, "excite.dat");
+  fprintf(fp, " %d\n", 8);
+  for (unsigned long n = 0; n < h->num_steps; n++)
+    fprintf(fp, full_precision ? "%23.16e\n" : "%16.8e\n", vh_waveform_value(h, n * h->dt, 0, 0.0));
+  fclose(fp);
+
+  /* process.dat. */
+  fp = fopen("process.dat", "w");
+  if (!fp) return bin_fail(h, "process.dat");
+  double mesh_size = h->dt * (2.0 * h->c0);
+  double fstart = 0.0;
+  double fstep = 1.0 / (h->num_steps * h->dt);
+  double fstop = h->num_steps * fstep;
+  char comment[70] = "";
+  snprintf(comment, sizeof comment - 1, "%s", h->comment);
+  fprintf(fp, "CE %s\n", comment);
+  fprintf(fp, "%lu\n", (unsigned long)nbin_obs);
+  for (int o = 0; o < h->num_obs; o++) {
+    vh_observer *ob = &h->obs[o];
+    if (ob->kind != OBS_TD_BINARY) continue;
+    for (int a = 0; a < 3; a++)
+      fprintf(fp, " %d %d %d", ob->gbbox[2 * a] - h->gibox[2 * a], ob->gbbox[2 * a + 1] - h->gibox[2 * a],
+              ob->step[a]);
+    fprintf(fp, "\n");
+  }
+  fprintf(fp, "%lu %lu\n", h->out_start + 1, h->out_stop + 1);
+  fprintf(fp, "%g %g %g\n", fstart, fstop, fstep);
+  fprintf(fp, "%g\n", mesh_size);
+  for (int a = 0; a < 3; a++)
+    fprintf(fp, " %d %d", first->gbbox[2 * a] - h->gibox[2 * a], first->gbbox[2 * a + 1] - h->gibox[2 * a]);
+  fprintf(fp, " %d\n", 1);
+  fclose(fp);
+  return 0;
+}
+
+/* A vgpu_bin_sink: one record per node and row -- i, j, k relative to the
+ * inner box as int, then Ex..Hz as float (src/observer.c:1164-1198). */
+void vhost_bin_sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows)
+{
+  vhost *h = user;
+  (void)first_row;
+  if (!h || !h->impulse || num_points != h->num_bin) {
+    if (h) h->impulse_failed = 1;
+    return;
+  }
+  enum { REC = 3 * 4 + 6 * 4 };
+  unsigned char *buf = malloc((size_t)num_points * REC);
+  if (!buf) { h->impulse_failed = 1; return; }
+  for (uint32_t r = 0; r < num_rows; r++) {
+    const float *row = rows + (size_t)r * num_points * 6;
+    for (int64_t q = 0; q < num_points; q++) {
+      int32_t ijk[3] = { h->bin_points[3 * q] - h->gibox[XLO], h->bin_points[3 * q + 1] - h->gibox[YLO],
+                         h->bin_points[3 * q + 2] - h->gibox[ZLO] };
+      memcpy(buf + q * REC, ijk, sizeof ijk);
+      memcpy(buf + q * REC + sizeof ijk, row + q * 6, 6 * sizeof(float));
+    }
+    if (fwrite(buf, REC, (size_t)num_points, h->impulse) != (size_t)num_points) h->impulse_failed = 1;
+  }
+  free(buf);
+}
+
+/* Close impulse.dat (src/observer.c:1201-1212). */
+int vhost_bin_end(vhost *h)
+{
+  if (!h) { vh_set_tls_error("null host handle"); return VGPU_EINVAL; }
+  int failed = h->impulse_failed;
+  if (h->impulse && fclose(h->impulse) != 0) failed = 1;
+  h->impulse = NULL;
+  h->impulse_failed = 0;
+  if (failed) {
+    vh_fail(h, "*** Error: writing impulse.dat failed");
+    vh_set_tls_error(h->err);
+    return VGPU_EINVAL;
+  }
+  return 0;
+}

@@ -326,6 +326,8 @@ int vh_build_problem(vh_ctx *c, int precision)
   p->td_points = c->td_points;
   p->num_fd = c->num_fd;
   p->fd_points = c->fd_points;
+  p->num_bin = c->num_bin;
+  p->bin_points = c->bin_points;
   p->num_freq = (int32_t)c->num_freq;
   p->omega = c->omega;
   c->prob_ready = 1;
@@ -351,6 +353,7 @@ uint64_t vhost_num_output_steps(const vhost *h)
 }
 int32_t vhost_num_td(const vhost *h) { return h->num_td; }
 int32_t vhost_num_fd(const vhost *h) { return h->num_fd; }
+int64_t vhost_num_bin(const vhost *h) { return h->num_bin; }
 int32_t vhost_num_freq(const vhost *h) { return (int32_t)h->num_freq; }
 double vhost_dt(const vhost *h) { return h->dt; }
 uint64_t vhost_num_cells(const vhost *h)
@@ -392,7 +395,8 @@ void vhost_free(vhost *c)
   free(c->wfs); free(c->srcs); free(c->pws); free(c->obs);
   free(c->debye_flim); free(c->debye_medium);
   free(c->sibc_pr); free(c->sibcs); free(c->sibc_rc); free(c->sibc_q); free(c->hops);
-  free(c->omega); free(c->td_points); free(c->fd_points);
+  free(c->omega); free(c->td_points); free(c->fd_points); free(c->bin_points);
+  if (c->impulse) fclose(c->impulse);
   free(c->p_srcs); free(c->p_src_vals); free(c->p_debye); free(c->p_debye_coef);
   free(c->p_pws); free(c->p_pw_vals); free(c->p_wfs); free(c->p_sibc);
   free(c);

@@ -496,5 +496,35 @@ int vh_init_observers(vh_ctx *c)
   c->omega = calloc(c->num_freq ? c->num_freq : 1, sizeof(double));
   for (unsigned long f = 0; f < c->num_freq; f++)
     c->omega[f] = 2.0 * c->pi * (c->start_freq + (int)f * c->step_freq);
+
+  /* Binary observers: their nodes in impulse.dat order, k outermost, then j,
+   * then i (src/observer.c:1172-1174).  A zero step never advances the
+   * reference's loop; it is refused here. */
+  int64_t nbin = 0;
+  for (int o = 0; o < c->num_obs; o++) {
+    vh_observer *ob = &c->obs[o];
+    if (ob->kind != OBS_TD_BINARY) continue;
+    for (int a = 0; a < 3; a++)
+      if (ob->step[a] <= 0)
+        return vh_fail(c, "*** Error: binary observer %s has a zero step along %c", ob->name, "xyz"[a]);
+    nbin += (int64_t)(1 + (ob->gbbox[ZHI] - ob->gbbox[ZLO]) / ob->step[2]) *
+            (1 + (ob->gbbox[YHI] - ob->gbbox[YLO]) / ob->step[1]) * (1 + (ob->gbbox[XHI] - ob->gbbox[XLO]) / ob->step[0]);
+  }
+  c->num_bin = nbin;
+  c->bin_points = calloc(3 * (size_t)(nbin ? nbin : 1), sizeof(int32_t));
+  if (!c->bin_points) return vh_fail(c, "*** Error: out of memory for binary observers");
+  int64_t q = 0;
+  for (int o = 0; o < c->num_obs; o++) {
+    vh_observer *ob = &c->obs[o];
+    if (ob->kind != OBS_TD_BINARY) continue;
+    for (int k = ob->gbbox[ZLO]; k <= ob->gbbox[ZHI]; k += ob->step[2])
+      for (int j = ob->gbbox[YLO]; j <= ob->gbbox[YHI]; j += ob->step[1])
+        for (int i = ob->gbbox[XLO]; i <= ob->gbbox[XHI]; i += ob->step[0]) {
+          c->bin_points[3 * q] = i;
+          c->bin_points[3 * q + 1] = j;
+          c->bin_points[3 * q + 2] = k;
+          q++;
+        }
+  }
   return 0;
 }

@@ -70,6 +70,11 @@ class Mesh:
         return int(N.lib().vhost_num_fd(self._h))
 
     @property
+    def num_bin(self) -> int:
+        """Nodes over all TDOM_BINARY observers."""
+        return int(N.lib().vhost_num_bin(self._h))
+
+    @property
     def num_freq(self) -> int:
         return int(N.lib().vhost_num_freq(self._h))
 
@@ -100,6 +105,34 @@ class Mesh:
                                                      re.ctypes.data, im.ctypes.data, int(full_precision)))
 
 
+    def write_lines(self, directory):
+        """xlines.dat / ylines.dat / zlines.dat, as the reference's set-up writes them."""
+        Path(directory).mkdir(parents=True, exist_ok=True)
+        with _chdir(directory):
+            N.check_host(N.lib().vhost_write_lines(self._h))
+
+    def bin_begin(self, directory, full_precision=False):
+        """impulse.dat header, excite.dat and process.dat (no-op without binary observers)."""
+        Path(directory).mkdir(parents=True, exist_ok=True)
+        with _chdir(directory):
+            N.check_host(N.lib().vhost_bin_begin(self._h, int(full_precision)))
+
+    def bin_append(self, rows):
+        """Append binary-observer rows [n][num_bin][6] (float32) to impulse.dat."""
+        r = np.ascontiguousarray(rows, dtype=np.float32)
+        if r.size:
+            N.lib().vhost_bin_sink(self._h, 0, r.shape[0], self.num_bin, r.ctypes.data)
+
+    def bin_end(self):
+        N.check_host(N.lib().vhost_bin_end(self._h))
+
+    def write_binary(self, directory, rows, full_precision=False):
+        """All binary-observer files from rows sampled elsewhere."""
+        self.bin_begin(directory, full_precision)
+        self.bin_append(rows)
+        self.bin_end()
+
+
 class GpuRun:
     """An engine instance on the current CUDA device (vgpu_create/run)."""
 
@@ -114,6 +147,35 @@ class GpuRun:
         n = self.mesh.num_steps - self.step if nsteps is None else nsteps
         N.check_gpu(N.lib().vgpu_run(self._e, n))
         return self
+
+    def collect_bin(self):
+        """Keep every binary-observer row the engine delivers (see bin())."""
+        self._bin_rows = []
+        npts = self.mesh.num_bin
+
+        def sink(user, first_row, num_rows, num_points, rows):
+            a = np.ctypeslib.as_array(rows, shape=(num_rows * num_points * 6,))
+            self._bin_rows.append((first_row, a.reshape(num_rows, num_points, 6).copy()))
+
+        self._bin_cb = N.BIN_SINK(sink)
+        N.check_gpu(N.lib().vgpu_set_bin_sink(self._e, C.cast(self._bin_cb, C.c_void_p), None))
+        self._bin_npts = npts
+        return self
+
+    def stream_bin_to(self, mesh: Mesh):
+        """Send binary-observer rows straight to the mesh's impulse.dat writer."""
+        fn = C.cast(N.lib().vhost_bin_sink, C.c_void_p)
+        N.check_gpu(N.lib().vgpu_set_bin_sink(self._e, fn, mesh._h))
+        return self
+
+    def bin(self):
+        """Collected rows [rows][num_bin][6] float32, in delivery order."""
+        if not getattr(self, "_bin_rows", None):
+            return np.zeros((0, self.mesh.num_bin, 6), dtype=np.float32)
+        return np.concatenate([r for _, r in self._bin_rows], axis=0)
+
+    def bin_first_rows(self):
+        return [f for f, _ in getattr(self, "_bin_rows", [])]
 
     @property
     def step(self) -> int:
@@ -174,7 +236,13 @@ class GpuRun:
 def run_mesh(mesh_path, out_dir, precision="fp64", full_precision=False):
     """The reference's command-line flow on the GPU: set up, propagate, write outputs."""
     m = Mesh(mesh_path)
-    g = GpuRun(m, precision).run()
+    m.write_lines(out_dir)
+    m.bin_begin(out_dir, full_precision)
+    g = GpuRun(m, precision)
+    if m.num_bin:
+        g.stream_bin_to(m)
+    g.run()
+    m.bin_end()
     re, im = g.dft()
     m.write_outputs(out_dir, g.td(), re, im, full_precision)
     g.close()
