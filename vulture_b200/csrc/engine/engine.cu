@@ -17,6 +17,9 @@
 #include <mutex>
 
 #include "kernels.cuh"
+#include "sweep_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 using namespace vgpu_dev;
 
@@ -154,11 +157,20 @@ struct Engine : EngineBase {
     uint64_t row0;
     uint32_t nrows;
   } bin_blk[2] = {};
+  // TMA sweeps: tile lists per launch (bulk, PML with 32-wide and 8-wide
+  // k rows), tensor maps per sweep and row width, full-volume UPML state.
+  struct SweepLaunch {
+    SweepTile *tiles = nullptr;
+    int ntiles = 0, grid = 0;
+    uint32_t smem = 0;
+  };
+  SweepLaunch sw_e[3], sw_h[3];   // [0] bulk, [1] PML KW=32, [2] PML KW=8
+  SweepMaps maps_e32{}, maps_e8{}, maps_h32{}, maps_h8{};
+  PmlFull<T> pfe{}, pfh{};
+  int pml_face[6] = {};
+  int *d_err = nullptr;
   // fused sweeps
   CoefIndex cie{}, cih{};
-  // Tile lists: bulk tiles first, then the PML regions' tiles.
-  Tile *d_tiles_e = nullptr, *d_tiles_h = nullptr;
-  int nbulk_e = 0, nbulk_h = 0, npml_e = 0, npml_h = 0;
   // graph
   cudaGraphExec_t graph = nullptr;
   uint64_t launches_per_step = 0;
@@ -257,8 +269,8 @@ struct Engine : EngineBase {
     if (int rc = setup_planewaves()) return rc;
     setup_ghost();
     if (int rc = setup_observers()) return rc;
-    if (int rc = setup_tiles()) return rc;
     if (int rc = setup_coef_index()) return rc;
+    if (int rc = setup_sweeps()) return rc;
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
     stats.device_bytes = mem.bytes;
@@ -283,16 +295,10 @@ struct Engine : EngineBase {
     for (int r = 0; r < 6; r++) {
       if (!p.pml_present[r]) continue;
       int q = pv.nreg++;
+      pml_face[q] = r;
       Box bb[6];
       for (int f = 0; f < 6; f++) bb[f] = box_from(p.pml_flim[r][f]);
       for (int f = 0; f < 6; f++) pv.lim[q][f] = bb[f];
-      for (int c = 0; c < 3; c++) {
-        int64_t ne = bb[c].count(), nh = bb[3 + c].count();
-        if (mem.alloc(&pv.PP[q][c], ne) || mem.alloc(&pv.P[q][c], ne) || mem.alloc(&pv.B[q][c], nh)) return VGPU_ENOMEM;
-        CK(cudaMemset(pv.PP[q][c], 0, sizeof(T) * (ne ? ne : 1)));
-        CK(cudaMemset(pv.P[q][c], 0, sizeof(T) * (ne ? ne : 1)));
-        CK(cudaMemset(pv.B[q][c], 0, sizeof(T) * (nh ? nh : 1)));
-      }
     }
     has_pml = pv.nreg > 0;
     if (!has_pml) return 0;
@@ -570,41 +576,6 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  static void add_tiles(std::vector<Tile> &out, int region, const Box &u, int ti)
-  {
-    if (u.empty()) return;
-    int kstart = (u.k0 / 32) * 32;
-    for (int i = u.i0; i <= u.i1; i += ti)
-      for (int j = u.j0; j <= u.j1; j += 8)
-        for (int k = kstart; k <= u.k1; k += 32) out.push_back(Tile{ region, i, std::min(i + ti - 1, u.i1), j, k, 0 });
-  }
-
-  // Tile lists of the fused E and H sweeps: the bulk union box and each PML
-  // region's union box, i runs sized so the grid fills the GPU a few times.
-  int setup_tiles()
-  {
-    int64_t cells = (int64_t)ube.count();
-    int nsm = 148;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
-    int64_t target_tiles = (int64_t)nsm * 8 * 4;
-    int ti = (int)std::max<int64_t>(1, std::min<int64_t>(16, cells / (256 * target_tiles)));
-    std::vector<Tile> te, th;
-    add_tiles(te, -1, ube, ti);
-    add_tiles(th, -1, ubh, ti);
-    nbulk_e = (int)te.size();
-    nbulk_h = (int)th.size();
-    for (int r = 0; r < pv.nreg; r++) {
-      Box e3[3] = { pv.lim[r][0], pv.lim[r][1], pv.lim[r][2] };
-      Box h3[3] = { pv.lim[r][3], pv.lim[r][4], pv.lim[r][5] };
-      add_tiles(te, r, unite(e3), ti);
-      add_tiles(th, r, unite(h3), ti);
-    }
-    npml_e = (int)te.size() - nbulk_e;
-    npml_h = (int)th.size() - nbulk_h;
-    if (upload(&d_tiles_e, te.data(), te.size()) || upload(&d_tiles_h, th.data(), th.size())) return VGPU_ENOMEM;
-    return 0;
-  }
-
   // Distinct coefficient tuples per cell: (alpha, beta) x 3 for E and
   // gamma x 3 for H.  Up to 256 tuples compress to one byte per cell.
   int build_index(int first, int count, CoefIndex &out)
@@ -647,6 +618,219 @@ struct Engine : EngineBase {
     out.idx = d_idx;
     out.table = d_tab;
     out.ntab = (int)seen.size();
+    return 0;
+  }
+
+  // ---- TMA sweeps ------------------------------------------------------
+
+  static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+  {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fn) {
+      void *ptr = nullptr;
+      cudaDriverEntryPointQueryResult q{};
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess)
+        fn = (PFN_cuTensorMapEncodeTiled_v12000)ptr;
+    }
+    return fn;
+  }
+
+  // A 3-D map over one [n0][n1][n2p] volume with box (bx, by, 1).
+  int make_map(CUtensorMap *m, const void *base, CUtensorMapDataType dt, int esize, int bx, int by)
+  {
+    auto fn = encode_fn();
+    if (!fn) return set_err(VGPU_ECUDA, "cuTensorMapEncodeTiled is not available");
+    cuuint64_t dims[3] = { (cuuint64_t)n2p, (cuuint64_t)p.n[1], (cuuint64_t)p.n[0] };
+    cuuint64_t strides[2] = { (cuuint64_t)n2p * esize, (cuuint64_t)n2p * p.n[1] * esize };
+    cuuint32_t box[3] = { (cuuint32_t)bx, (cuuint32_t)by, 1 };
+    cuuint32_t es[3] = { 1, 1, 1 };
+    CUresult r = fn(m, dt, 3, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(VGPU_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+  }
+
+  // Maps of one sweep: own = the updated components, oth = the curl's.
+  int make_sweep_maps(SweepMaps &m, bool esweep, int kw)
+  {
+    const int jh = 256 / kw, w = kw + 16 / (int)sizeof(T);
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const int e = (int)sizeof(T);
+    for (int c = 0; c < 3; c++) {
+      if (int rc = make_map(&m.own[c], g.F[(esweep ? EX : HX) + c], dt, e, w, jh)) return rc;
+      if (int rc = make_map(&m.oth[c], g.F[(esweep ? HX : EX) + c], dt, e, w, jh + 1)) return rc;
+    }
+    const int ncoef = esweep ? 6 : 3;
+    for (int c = 0; c < ncoef; c++)
+      if (int rc = make_map(&m.coef[c], g.cf[(esweep ? 0 : 6) + c], dt, e, w, jh)) return rc;
+    const CoefIndex &ci = esweep ? cie : cih;
+    if (ci.idx)
+      if (int rc = make_map(&m.idx, ci.idx, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, 32, jh)) return rc;
+    if (has_pml) {
+      const PmlFull<T> &pf = esweep ? pfe : pfh;
+      for (int c = 0; c < (esweep ? 6 : 3); c++)
+        if (int rc = make_map(&m.aux[c], pf.aux[c], dt, e, w, jh)) return rc;
+    }
+    return 0;
+  }
+
+  // Tiles of kw (k) x 256/kw (j) columns over box u, i runs of ti planes.
+  static void add_sweep_tiles(std::vector<SweepTile> &out, int region, const Box &u, int ti, int kw)
+  {
+    if (u.empty()) return;
+    const int jh = 256 / kw;
+    const int kstart = kw == 32 ? (u.k0 / 32) * 32 : u.k0;
+    for (int i = u.i0; i <= u.i1; i += ti)
+      for (int j = u.j0; j <= u.j1; j += jh)
+        for (int k = kstart; k <= u.k1; k += kw)
+          out.push_back(SweepTile{ region, i, std::min(i + ti - 1, u.i1), j, k });
+  }
+
+  template <int KW, bool ES, bool PML>
+  int prepare_launch(SweepLaunch &L, const std::vector<SweepTile> &tiles, bool compressed)
+  {
+    L.ntiles = (int)tiles.size();
+    if (!L.ntiles) return 0;
+    if (upload(&L.tiles, tiles.data(), tiles.size())) return VGPU_ENOMEM;
+    L.smem = SweepLayout<T, KW, ES, PML>::smem_bytes(compressed);
+    auto kern = k_sweep_tma<T, KW, ES, PML>;
+    // The attribute is per kernel, shared by every engine in the process:
+    // set it to the larger (uncompressed) layout.
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)SweepLayout<T, KW, ES, PML>::smem_bytes(false)));
+    int per_sm = 0, nsm = 148;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, L.smem));
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    if (per_sm < 1) return set_err(VGPU_ECUDA, "sweep kernel does not fit on an SM (%u bytes of shared memory)", L.smem);
+    L.grid = std::min(L.ntiles, per_sm * nsm);
+    return 0;
+  }
+
+  // Regions of one component must be disjoint from each other and from the
+  // bulk box, so that full-volume auxiliaries hold each point's own state.
+  int check_disjoint()
+  {
+    for (int f = 0; f < 6; f++) {
+      const Box &bulk = f < 3 ? be[f] : bh[f - 3];
+      for (int a = 0; a < pv.nreg; a++) {
+        const Box &x = pv.lim[a][f];
+        if (x.empty()) continue;
+        auto meet = [](const Box &u, const Box &v) {
+          return !u.empty() && !v.empty() && u.i0 <= v.i1 && v.i0 <= u.i1 && u.j0 <= v.j1 && v.j0 <= u.j1 &&
+                 u.k0 <= v.k1 && v.k0 <= u.k1;
+        };
+        if (meet(x, bulk)) return set_err(VGPU_EINVAL, "PML region %d overlaps the bulk limits of field %d", a, f);
+        for (int b = a + 1; b < pv.nreg; b++)
+          if (meet(x, pv.lim[b][f])) return set_err(VGPU_EINVAL, "PML regions %d and %d overlap for field %d", a, b, f);
+      }
+    }
+    return 0;
+  }
+
+  int setup_sweeps()
+  {
+    if (mem.alloc(&d_err, 1)) return VGPU_ENOMEM;
+    CK(cudaMemset(d_err, 0, sizeof(int)));
+    if (has_pml) {
+      if (int rc = check_disjoint()) return rc;
+      T *aux = nullptr;
+      if (mem.alloc(&aux, (size_t)vol * 9)) return VGPU_ENOMEM;
+      CK(cudaMemset(aux, 0, sizeof(T) * vol * 9));
+      for (int c = 0; c < 6; c++) pfe.aux[c] = aux + (int64_t)c * vol;
+      for (int c = 0; c < 3; c++) pfh.aux[c] = aux + (int64_t)(6 + c) * vol;
+      for (PmlFull<T> *pf : { &pfe, &pfh }) {
+        for (int a = 0; a < 3; a++) {
+          pf->ad[a] = pv.ad[a]; pf->bd[a] = pv.bd[a]; pf->ah[a] = pv.ah[a];
+          pf->bh[a] = pv.bh[a]; pf->ibd[a] = pv.ibd[a]; pf->ibh[a] = pv.ibh[a];
+        }
+      }
+      for (int q = 0; q < pv.nreg; q++)
+        for (int c = 0; c < 3; c++) {
+          pfe.lim[q][c] = pv.lim[q][EX + c];
+          pfh.lim[q][c] = pv.lim[q][HX + c];
+        }
+    }
+    // Tiles: i runs sized so each launch has several tiles per resident
+    // block, for balance; the pipeline runs across tile boundaries.
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    auto run_len = [&](int64_t cells) {
+      int64_t t = cells / (256LL * nsm * 16);
+      return (int)std::max<int64_t>(4, std::min<int64_t>(32, t));
+    };
+    for (int es = 0; es < 2; es++) {
+      const Box &ub = es ? ube : ubh;
+      std::vector<SweepTile> bulk, p32, p8;
+      add_sweep_tiles(bulk, -1, ub, run_len(ub.count()), 32);
+      for (int q = 0; q < pv.nreg; q++) {
+        Box c3[3] = { pv.lim[q][es ? EX : HX], pv.lim[q][es ? EY : HY], pv.lim[q][es ? EZ : HZ] };
+        Box u = unite(c3);
+        if (u.i1 < u.i0) continue;
+        if (pml_face[q] / 2 == 2)
+          add_sweep_tiles(p8, q, u, run_len(u.count()), 8);
+        else
+          add_sweep_tiles(p32, q, u, run_len(u.count()), 32);
+      }
+      SweepLaunch *L = es ? sw_e : sw_h;
+      bool comp = (es ? cie : cih).idx != nullptr;
+      if (es) {
+        if (int rc = prepare_launch<32, true, false>(L[0], bulk, comp)) return rc;
+        if (int rc = prepare_launch<32, true, true>(L[1], p32, comp)) return rc;
+        if (int rc = prepare_launch<8, true, true>(L[2], p8, comp)) return rc;
+      } else {
+        if (int rc = prepare_launch<32, false, false>(L[0], bulk, comp)) return rc;
+        if (int rc = prepare_launch<32, false, true>(L[1], p32, comp)) return rc;
+        if (int rc = prepare_launch<8, false, true>(L[2], p8, comp)) return rc;
+      }
+    }
+    if (int rc = make_sweep_maps(maps_e32, true, 32)) return rc;
+    if (int rc = make_sweep_maps(maps_h32, false, 32)) return rc;
+    if (int rc = make_sweep_maps(maps_e8, true, 8)) return rc;
+    if (int rc = make_sweep_maps(maps_h8, false, 8)) return rc;
+    return 0;
+  }
+
+  // Launch the sweeps of one half step: which = 0 bulk, 1 PML (both row
+  // widths).  Returns the number of kernels launched through `count`.
+  int launch_sweeps(bool esweep, int which, uint64_t *count)
+  {
+    const dim3 blk(256);
+    SweepLaunch *L = esweep ? sw_e : sw_h;
+    const Box *bb = esweep ? be : bh;
+    const CoefIndex &ci = esweep ? cie : cih;
+    const PmlFull<T> &pf = esweep ? pfe : pfh;
+    if (which == 0 && L[0].ntiles) {
+      if (esweep)
+        k_sweep_tma<T, 32, true, false><<<L[0].grid, blk, L[0].smem, s>>>(maps_e32, g, L[0].tiles, L[0].ntiles, bb[0],
+                                                                          bb[1], bb[2], pf, ci, d_err);
+      else
+        k_sweep_tma<T, 32, false, false><<<L[0].grid, blk, L[0].smem, s>>>(maps_h32, g, L[0].tiles, L[0].ntiles, bb[0],
+                                                                           bb[1], bb[2], pf, ci, d_err);
+      if (count) ++*count;
+    }
+    if (which == 1) {
+      if (L[1].ntiles) {
+        if (esweep)
+          k_sweep_tma<T, 32, true, true><<<L[1].grid, blk, L[1].smem, s>>>(maps_e32, g, L[1].tiles, L[1].ntiles, bb[0],
+                                                                           bb[1], bb[2], pf, ci, d_err);
+        else
+          k_sweep_tma<T, 32, false, true><<<L[1].grid, blk, L[1].smem, s>>>(maps_h32, g, L[1].tiles, L[1].ntiles, bb[0],
+                                                                            bb[1], bb[2], pf, ci, d_err);
+        if (count) ++*count;
+      }
+      if (L[2].ntiles) {
+        if (esweep)
+          k_sweep_tma<T, 8, true, true><<<L[2].grid, blk, L[2].smem, s>>>(maps_e8, g, L[2].tiles, L[2].ntiles, bb[0],
+                                                                          bb[1], bb[2], pf, ci, d_err);
+        else
+          k_sweep_tma<T, 8, false, true><<<L[2].grid, blk, L[2].smem, s>>>(maps_h8, g, L[2].tiles, L[2].ntiles, bb[0],
+                                                                           bb[1], bb[2], pf, ci, d_err);
+        if (count) ++*count;
+      }
+    }
     return 0;
   }
 
@@ -711,6 +895,15 @@ struct Engine : EngineBase {
       CK(cudaEventCreateWithFlags(&ev_fill[q], cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&ev_copy[q], cudaEventDisableTiming));
     }
+    return 0;
+  }
+
+  // A sweep block whose pipeline wait ran out leaves a code in d_err.
+  int check_device_error()
+  {
+    int h = 0;
+    CK(cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return set_err(VGPU_ETIMEOUT, "a sweep's shared-memory pipeline timed out waiting for its loads");
     return 0;
   }
 
@@ -885,6 +1078,7 @@ struct Engine : EngineBase {
     }
     CK(cudaEventRecord(e1, s));
     CK(cudaEventSynchronize(e1));
+    if (int rc = check_device_error()) return rc;
     if (p.num_bin > 0) {
       // The older pending block first.
       int a = 0, b = 1;
@@ -942,21 +1136,15 @@ struct Engine : EngineBase {
   // error (profiling), otherwise it launches nothing.
   int launch_one(int kernel, bool required = true, uint64_t *count = nullptr)
   {
-    const dim3 blk(32, 8);
-    if (kernel == VGPU_K_BULK_E && nbulk_e) {
-      k_sweep_e<T, false><<<nbulk_e, blk, 0, s>>>(g, d_tiles_e, be[0], be[1], be[2], pv, cie);
-    } else if (kernel == VGPU_K_BULK_H && nbulk_h) {
-      k_sweep_h<T, false><<<nbulk_h, blk, 0, s>>>(g, d_tiles_h, bh[0], bh[1], bh[2], pv, cih);
-    } else if (kernel == VGPU_K_PML_E && npml_e) {
-      k_sweep_e<T, true><<<npml_e, blk, 0, s>>>(g, d_tiles_e + nbulk_e, be[0], be[1], be[2], pv, cie);
-    } else if (kernel == VGPU_K_PML_H && npml_h) {
-      k_sweep_h<T, true><<<npml_h, blk, 0, s>>>(g, d_tiles_h + nbulk_h, bh[0], bh[1], bh[2], pv, cih);
-    } else {
+    const bool es = kernel == VGPU_K_BULK_E || kernel == VGPU_K_PML_E;
+    const int which = (kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) ? 0 : 1;
+    const SweepLaunch *L = es ? sw_e : sw_h;
+    const bool present = which == 0 ? L[0].ntiles > 0 : (L[1].ntiles + L[2].ntiles) > 0;
+    if (kernel < 0 || kernel > 3 || !present) {
       if (!required) return 0;
       return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
     }
-    if (count) ++*count;
-    return 0;
+    return launch_sweeps(es, which, count);
   }
 
   int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override

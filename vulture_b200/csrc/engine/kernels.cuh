@@ -47,9 +47,8 @@ struct Grid {
 };
 
 // ---------------------------------------------------------------------------
-// UPML state (src/pml.c:44-84): 1-D profiles per axis, each region's field
-// limits and its auxiliary arrays PP, P (E) and B (H), stored [i][j][k] over
-// the component's limits.
+// UPML state (src/pml.c:44-84): 1-D profiles per axis and each region's
+// field limits.  The auxiliary fields live in full volumes (sweep_tma.cuh).
 // ---------------------------------------------------------------------------
 
 template <typename T>
@@ -57,31 +56,6 @@ struct PmlView {
   const T *ad[3], *bd[3], *ah[3], *bh[3], *ibd[3], *ibh[3];
   int nreg;
   Box lim[6][6];       // [region][field]
-  T *PP[6][3], *P[6][3], *B[6][3];
-};
-
-__device__ __forceinline__ int64_t aux_index(const Box &l, int i, int j, int k)
-{
-  return ((int64_t)(i - l.i0) * l.nj() + (j - l.j0)) * l.nk() + (k - l.k0);
-}
-
-// ---------------------------------------------------------------------------
-// Sweeps: the bulk update (src/grid.c:709-888) and the UPML update of every
-// region (src/pml.c:859-1176).  The host cuts the bulk union box and each PML
-// region's union box
-// into tiles of 32 (k) x 8 (j) columns and a run of i planes; one block per
-// tile, one thread per (j,k) column marching along i.  Values of the previous
-// plane (E sweep) or the next plane (H sweep) stay in registers; the j and k
-// neighbours are re-read through L1, so each field value comes from DRAM
-// about once per sweep.  Arithmetic is the reference's expression, in the
-// reference's order.
-// ---------------------------------------------------------------------------
-
-struct Tile {
-  int region;      // -1: bulk, 0..5: PML region
-  int i0, i1;      // planes marched (inclusive)
-  int j0, k0;      // first column of the 8 x 32 tile
-  int pad;
 };
 
 template <typename T>
@@ -97,227 +71,6 @@ struct CoefIndex {
   int ntab;
 };
 
-// Clamp (i,j,k) into a box; used so that auxiliary-array loads stay in
-// bounds for columns whose store is predicated off.
-__device__ __forceinline__ int64_t aux_index_clamped(const Box &l, int i, int j, int k)
-{
-  i = min(max(i, l.i0), l.i1);
-  j = min(max(j, l.j0), l.j1);
-  k = min(max(k, l.k0), l.k1);
-  return aux_index(l, i, j, k);
-}
-
-// Each plane of a sweep first issues every load it needs -- fields at
-// clamped (always in-bounds) addresses, coefficients, UPML auxiliaries --
-// and only then computes and stores, each store predicated on its
-// component's box.  Loads thus overlap in flight instead of waiting on the
-// previous component's store.
-template <typename T, bool PML>
-__device__ __forceinline__ void sweep_e_tile(const Grid<T> &g, const Tile &t, const Box &b0, const Box &b1,
-                                             const Box &b2, const PmlView<T> &pv, const CoefIndex &ci, const T *tab)
-{
-  const int k = t.k0 + threadIdx.x;
-  const int j = t.j0 + threadIdx.y;
-  const bool jok = j < g.n1;
-  const int jc = jok ? j : g.n1 - 1;
-  const int64_t dj = jc > 0 ? g.s1 : 0;  // offset of (j-1), clamped at 0
-  const int64_t dk = k > 0 ? 1 : 0;      // offset of (k-1), clamped at 0
-  T *__restrict__ Ex = g.F[EX];
-  T *__restrict__ Ey = g.F[EY];
-  T *__restrict__ Ez = g.F[EZ];
-  const T *__restrict__ Hx = g.F[HX];
-  const T *__restrict__ Hy = g.F[HY];
-  const T *__restrict__ Hz = g.F[HZ];
-  const T idhy = ld(g.idh[1] + jc);
-  const T idhz = ld(g.idh[2] + k);
-  int64_t x = g.at(max(t.i0 - 1, 0), jc, k);
-  T hy_prev = ld(Hy + x);
-  T hz_prev = ld(Hz + x);
-  if (t.i0 == 0) x -= g.s0;
-  for (int i = t.i0; i <= t.i1; i++) {
-    x += g.s0;
-    const T hx = ld(Hx + x), hy = ld(Hy + x), hz = ld(Hz + x);
-    const T hx_jm = ld(Hx + x - dj), hz_jm = ld(Hz + x - dj);
-    const T hx_km = ld(Hx + x - dk), hy_km = ld(Hy + x - dk);
-    const T idhx = ld(g.idh[0] + i);
-    T al0, al1, al2, be0, be1, be2;
-    if (ci.idx) {
-      const T *cw = tab + 6 * (int)ci.idx[x];
-      al0 = cw[0]; al1 = cw[1]; al2 = cw[2];
-      be0 = cw[3]; be1 = cw[4]; be2 = cw[5];
-    } else {
-      al0 = ld(g.cf[0] + x); al1 = ld(g.cf[1] + x); al2 = ld(g.cf[2] + x);
-      be0 = ld(g.cf[3] + x); be1 = ld(g.cf[4] + x); be2 = ld(g.cf[5] + x);
-    }
-    const T ex = Ex[x], ey = Ey[x], ez = Ez[x];
-    const bool s0 = jok && b0.contains(i, j, k);
-    const bool s1 = jok && b1.contains(i, j, k);
-    const bool s2 = jok && b2.contains(i, j, k);
-    const T c0 = idhy * (hz - hz_jm) + idhz * (hy_km - hy);
-    const T c1 = idhz * (hx - hx_km) + idhx * (hz_prev - hz);
-    const T c2 = idhx * (hy - hy_prev) + idhy * (hx_jm - hx);
-    if (!PML) {
-      if (s0) Ex[x] = al0 * ex + be0 * c0;
-      if (s1) Ey[x] = al1 * ey + be1 * c1;
-      if (s2) Ez[x] = al2 * ez + be2 * c2;
-    } else {
-      const int r = t.region;
-      const int64_t a0 = aux_index_clamped(b0, i, jc, k);
-      const int64_t a1 = aux_index_clamped(b1, i, jc, k);
-      const int64_t a2 = aux_index_clamped(b2, i, jc, k);
-      const bool h0 = !b0.empty(), h1 = !b1.empty(), h2 = !b2.empty();
-      T *PP0 = pv.PP[r][0], *P0 = pv.P[r][0];
-      T *PP1 = pv.PP[r][1], *P1 = pv.P[r][1];
-      T *PP2 = pv.PP[r][2], *P2 = pv.P[r][2];
-      const T oPP0 = h0 ? PP0[a0] : (T)0, oP0 = h0 ? P0[a0] : (T)0;
-      const T oPP1 = h1 ? PP1[a1] : (T)0, oP1 = h1 ? P1[a1] : (T)0;
-      const T oPP2 = h2 ? PP2[a2] : (T)0, oP2 = h2 ? P2[a2] : (T)0;
-      const T ad0 = ld(pv.ad[0] + i), bd0 = ld(pv.bd[0] + i), ah0 = ld(pv.ah[0] + i), ibh0 = ld(pv.ibh[0] + i);
-      const T ad1 = ld(pv.ad[1] + jc), bd1 = ld(pv.bd[1] + jc), ah1 = ld(pv.ah[1] + jc), ibh1 = ld(pv.ibh[1] + jc);
-      const T ad2 = ld(pv.ad[2] + k), bd2 = ld(pv.bd[2] + k), ah2 = ld(pv.ah[2] + k), ibh2 = ld(pv.ibh[2] + k);
-      if (s0) {
-        const T nPP = al0 * oPP0 + be0 * c0;
-        PP0[a0] = nPP;
-        const T nP = ad1 * oP0 + bd1 * (nPP - oPP0);
-        P0[a0] = nP;
-        Ex[x] = ad2 * ex + bd2 * ibh0 * (nP - ah0 * oP0);
-      }
-      if (s1) {
-        const T nPP = al1 * oPP1 + be1 * c1;
-        PP1[a1] = nPP;
-        const T nP = ad2 * oP1 + bd2 * (nPP - oPP1);
-        P1[a1] = nP;
-        Ey[x] = ad0 * ey + bd0 * ibh1 * (nP - ah1 * oP1);
-      }
-      if (s2) {
-        const T nPP = al2 * oPP2 + be2 * c2;
-        PP2[a2] = nPP;
-        const T nP = ad0 * oP2 + bd0 * (nPP - oPP2);
-        P2[a2] = nP;
-        Ez[x] = ad1 * ez + bd1 * ibh2 * (nP - ah2 * oP2);
-      }
-    }
-    hy_prev = hy;
-    hz_prev = hz;
-  }
-}
-
-// PML tiles carry more live values than bulk tiles, so they run as their
-// own launch with a larger register budget.
-template <typename T, bool PML>
-__global__ void __launch_bounds__(256, PML ? 2 : (sizeof(T) == 4 ? 4 : 3))
-    k_sweep_e(Grid<T> g, const Tile *__restrict__ tiles, Box bx, Box by, Box bz, PmlView<T> pv, CoefIndex ci)
-{
-  __shared__ T tab[256 * 6];
-  if (ci.idx) {
-    const T *src = (const T *)ci.table;
-    for (int q = threadIdx.y * 32 + threadIdx.x; q < ci.ntab * 6; q += 256) tab[q] = src[q];
-    __syncthreads();
-  }
-  const Tile t = tiles[blockIdx.x];
-  if (!PML)
-    sweep_e_tile<T, false>(g, t, bx, by, bz, pv, ci, tab);
-  else
-    sweep_e_tile<T, true>(g, t, pv.lim[t.region][EX], pv.lim[t.region][EY], pv.lim[t.region][EZ], pv, ci, tab);
-}
-
-template <typename T, bool PML>
-__device__ __forceinline__ void sweep_h_tile(const Grid<T> &g, const Tile &t, const Box &b0, const Box &b1,
-                                             const Box &b2, const PmlView<T> &pv, const CoefIndex &ci, const T *tab)
-{
-  const int k = t.k0 + threadIdx.x;
-  const int j = t.j0 + threadIdx.y;
-  const bool jok = j < g.n1;
-  const int jc = jok ? j : g.n1 - 1;
-  const int64_t dj = jc + 1 < g.n1 ? g.s1 : 0;  // offset of (j+1), clamped at n1-1
-  const int64_t dk = k + 1 < g.s1 ? 1 : 0;       // offset of (k+1), clamped at the row end
-  const T *__restrict__ Ex = g.F[EX];
-  const T *__restrict__ Ey = g.F[EY];
-  const T *__restrict__ Ez = g.F[EZ];
-  T *__restrict__ Hx = g.F[HX];
-  T *__restrict__ Hy = g.F[HY];
-  T *__restrict__ Hz = g.F[HZ];
-  const T idey = ld(g.ide[1] + jc);
-  const T idez = ld(g.ide[2] + k);
-  int64_t x = g.at(t.i0, jc, k);
-  T ey = ld(Ey + x);
-  T ez = ld(Ez + x);
-  for (int i = t.i0; i <= t.i1; i++) {
-    const int64_t di = i + 1 < g.n0 ? g.s0 : 0;  // offset of (i+1), clamped at n0-1
-    const T ex = ld(Ex + x);
-    const T ex_jp = ld(Ex + x + dj), ez_jp = ld(Ez + x + dj);
-    const T ex_kp = ld(Ex + x + dk), ey_kp = ld(Ey + x + dk);
-    const T ey_ip = ld(Ey + x + di), ez_ip = ld(Ez + x + di);
-    const T idex = ld(g.ide[0] + i);
-    T ga0, ga1, ga2;
-    if (ci.idx) {
-      const T *cw = tab + 3 * (int)ci.idx[x];
-      ga0 = cw[0]; ga1 = cw[1]; ga2 = cw[2];
-    } else {
-      ga0 = ld(g.cf[6] + x); ga1 = ld(g.cf[7] + x); ga2 = ld(g.cf[8] + x);
-    }
-    const T hx = Hx[x], hy = Hy[x], hz = Hz[x];
-    const bool s0 = jok && b0.contains(i, j, k);
-    const bool s1 = jok && b1.contains(i, j, k);
-    const bool s2 = jok && b2.contains(i, j, k);
-    const T c0 = idez * (ey_kp - ey) + idey * (ez - ez_jp);
-    const T c1 = idex * (ez_ip - ez) + idez * (ex - ex_kp);
-    const T c2 = idey * (ex_jp - ex) + idex * (ey - ey_ip);
-    if (!PML) {
-      if (s0) Hx[x] = hx + ga0 * c0;
-      if (s1) Hy[x] = hy + ga1 * c1;
-      if (s2) Hz[x] = hz + ga2 * c2;
-    } else {
-      const int r = t.region;
-      const int64_t a0 = aux_index_clamped(b0, i, jc, k);
-      const int64_t a1 = aux_index_clamped(b1, i, jc, k);
-      const int64_t a2 = aux_index_clamped(b2, i, jc, k);
-      const bool h0 = !b0.empty(), h1 = !b1.empty(), h2 = !b2.empty();
-      T *B0 = pv.B[r][0], *B1 = pv.B[r][1], *B2 = pv.B[r][2];
-      const T oB0 = h0 ? B0[a0] : (T)0, oB1 = h1 ? B1[a1] : (T)0, oB2 = h2 ? B2[a2] : (T)0;
-      const T ah0 = ld(pv.ah[0] + i), bh0 = ld(pv.bh[0] + i), ad0 = ld(pv.ad[0] + i), ibd0 = ld(pv.ibd[0] + i);
-      const T ah1 = ld(pv.ah[1] + jc), bh1 = ld(pv.bh[1] + jc), ad1 = ld(pv.ad[1] + jc), ibd1 = ld(pv.ibd[1] + jc);
-      const T ah2 = ld(pv.ah[2] + k), bh2 = ld(pv.bh[2] + k), ad2 = ld(pv.ad[2] + k), ibd2 = ld(pv.ibd[2] + k);
-      if (s0) {
-        const T nB = ah1 * oB0 + ga0 * bh1 * c0;
-        B0[a0] = nB;
-        Hx[x] = ah2 * hx + bh2 * ibd0 * (nB - ad0 * oB0);
-      }
-      if (s1) {
-        const T nB = ah2 * oB1 + ga1 * bh2 * c1;
-        B1[a1] = nB;
-        Hy[x] = ah0 * hy + bh0 * ibd1 * (nB - ad1 * oB1);
-      }
-      if (s2) {
-        const T nB = ah0 * oB2 + ga2 * bh0 * c2;
-        B2[a2] = nB;
-        Hz[x] = ah1 * hz + bh1 * ibd2 * (nB - ad2 * oB2);
-      }
-    }
-    ey = ey_ip;
-    ez = ez_ip;
-    x += g.s0;
-  }
-}
-
-// PML tiles carry more live values than bulk tiles, so they run as their
-// own launch with a larger register budget.
-template <typename T, bool PML>
-__global__ void __launch_bounds__(256, PML ? 2 : (sizeof(T) == 4 ? 4 : 3))
-    k_sweep_h(Grid<T> g, const Tile *__restrict__ tiles, Box bx, Box by, Box bz, PmlView<T> pv, CoefIndex ci)
-{
-  __shared__ T tab[256 * 3];
-  if (ci.idx) {
-    const T *src = (const T *)ci.table;
-    for (int q = threadIdx.y * 32 + threadIdx.x; q < ci.ntab * 3; q += 256) tab[q] = src[q];
-    __syncthreads();
-  }
-  const Tile t = tiles[blockIdx.x];
-  if (!PML)
-    sweep_h_tile<T, false>(g, t, bx, by, bz, pv, ci, tab);
-  else
-    sweep_h_tile<T, true>(g, t, pv.lim[t.region][HX], pv.lim[t.region][HY], pv.lim[t.region][HZ], pv, ci, tab);
-}
 
 // ---------------------------------------------------------------------------
 // Mur first-order ABC (src/mur.c:135-555).  A list of planar work items; each
