@@ -217,15 +217,18 @@ def run_gpu_arm(args):
     value = world * n_out * args.steps / (ms * 1e-3) / 1e6
 
     # Roofline of the dominant kernel, each sweep timed live on the engine's
-    # stream with CUDA events.
+    # stream with CUDA events.  Bytes: the algorithmic words of each point
+    # the launch updates, by the bulk or the UPML formula.
     kern = {}
-    for name, kid, words in (("k_sweep_e_bulk", N.VGPU_K_BULK_E, WORDS_E), ("k_sweep_h_bulk", N.VGPU_K_BULK_H, WORDS_H),
-                             ("k_sweep_e_pml", N.VGPU_K_PML_E, WORDS_PML_E),
-                             ("k_sweep_h_pml", N.VGPU_K_PML_H, WORDS_PML_H)):
+    for name, kid, wb, wp in (("k_sweep_e_bulk", N.VGPU_K_BULK_E, WORDS_E, WORDS_PML_E),
+                              ("k_sweep_h_bulk", N.VGPU_K_BULK_H, WORDS_H, WORDS_PML_H),
+                              ("k_sweep_e_pml", N.VGPU_K_PML_E, WORDS_E, WORDS_PML_E),
+                              ("k_sweep_h_pml", N.VGPU_K_PML_H, WORDS_H, WORDS_PML_H)):
         kms, pts = g.time_kernel(kid, warmup=3, iters=20)
-        cells = pts / 3.0
-        kern[name] = dict(ms=kms, cells=cells, bytes=words * B_ALG[prec] * cells,
-                          gbs=words * B_ALG[prec] * cells / (kms * 1e-3) / 1e9)
+        bp, pp = g.sweep_points(kid)
+        nbytes = (wb * bp + wp * pp) / 3.0 * B_ALG[prec]
+        kern[name] = dict(ms=kms, cells=pts / 3.0, bulk_points=bp, pml_points=pp, bytes=nbytes,
+                          gbs=nbytes / (kms * 1e-3) / 1e9)
     g.close()
     peak, peak_kind = peaks()
     dom = max(kern, key=lambda k: kern[k]["ms"])

@@ -286,8 +286,15 @@ int vgpu_check_finite(vgpu_engine *engine);
 
 uint64_t vgpu_current_step(const vgpu_engine *engine);
 
-/* Kernels of one time step, for vgpu_time_kernel. */
+/* Sweep kernels of one time step, for vgpu_time_kernel: the launch over
+ * tiles holding only bulk points, and the launch over the UPML regions'
+ * tiles (the X and Y regions' own, plus the bulk-footprint tiles whose rows
+ * reach into a Z region, which update bulk and UPML points together). */
 enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 };
+
+/* Field points one sweep kernel updates per launch with the bulk formula
+ * and with the UPML formula. */
+int vgpu_sweep_points(const vgpu_engine *engine, int32_t kernel, uint64_t *bulk_points, uint64_t *pml_points);
 
 /* Profiling hook: launch one of the step's kernels `iters` times on the
  * engine's stream (after `warmup` untimed launches) and report the mean

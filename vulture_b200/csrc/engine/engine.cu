@@ -76,6 +76,7 @@ struct EngineBase {
   virtual int write_field(int c, const double *in) = 0;
   virtual int check_finite() = 0;
   virtual int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) = 0;
+  virtual int sweep_points(int kernel, uint64_t *bulk_pts, uint64_t *pml_pts) = 0;
   vgpu_bin_sink bin_sink = nullptr;
   void *bin_user = nullptr;
   uint64_t step = 0;
@@ -157,15 +158,17 @@ struct Engine : EngineBase {
     uint64_t row0;
     uint32_t nrows;
   } bin_blk[2] = {};
-  // TMA sweeps: tile lists per launch (bulk, PML with 32-wide and 8-wide
-  // k rows), tensor maps per sweep and row width, full-volume UPML state.
+  // TMA sweeps: tile lists and headers per launch, tensor maps per sweep,
+  // full-volume UPML state.
   struct SweepLaunch {
     SweepTile *tiles = nullptr;
+    void *headers = nullptr;     // SweepHeader<T, PML>[ntiles]
     int ntiles = 0, grid = 0;
     uint32_t smem = 0;
+    uint64_t bulk_points = 0, pml_points = 0;   // field points one launch updates
   };
-  SweepLaunch sw_e[3], sw_h[3];   // [0] bulk, [1] PML KW=32, [2] PML KW=8
-  SweepMaps maps_e32{}, maps_e8{}, maps_h32{}, maps_h8{};
+  SweepLaunch sw_e[2], sw_h[2];   // [0] bulk tiles, [1] UPML and mixed tiles
+  SweepMaps maps_e{}, maps_h{};
   PmlFull<T> pfe{}, pfh{};
   int pml_face[6] = {};
   int *d_err = nullptr;
@@ -638,12 +641,14 @@ struct Engine : EngineBase {
     return fn;
   }
 
-  // A 3-D map over one [n0][n1][n2p] volume with box (bx, by, 1).
+  // A 3-D map over one [n0][n1][n2p] volume with box (bx, by, 1).  Its k
+  // extent is n2, not the padded row: columns past the grid read as zero
+  // without touching memory.
   int make_map(CUtensorMap *m, const void *base, CUtensorMapDataType dt, int esize, int bx, int by)
   {
     auto fn = encode_fn();
     if (!fn) return set_err(VGPU_ECUDA, "cuTensorMapEncodeTiled is not available");
-    cuuint64_t dims[3] = { (cuuint64_t)n2p, (cuuint64_t)p.n[1], (cuuint64_t)p.n[0] };
+    cuuint64_t dims[3] = { (cuuint64_t)p.n[2], (cuuint64_t)p.n[1], (cuuint64_t)p.n[0] };
     cuuint64_t strides[2] = { (cuuint64_t)n2p * esize, (cuuint64_t)n2p * p.n[1] * esize };
     cuuint32_t box[3] = { (cuuint32_t)bx, (cuuint32_t)by, 1 };
     cuuint32_t es[3] = { 1, 1, 1 };
@@ -654,14 +659,15 @@ struct Engine : EngineBase {
   }
 
   // Maps of one sweep: own = the updated components, oth = the curl's.
-  int make_sweep_maps(SweepMaps &m, bool esweep, int kw)
+  // Curl boxes carry a 16-byte halo column; the others are one tile row.
+  int make_sweep_maps(SweepMaps &m, bool esweep)
   {
-    const int jh = 256 / kw, w = kw + 16 / (int)sizeof(T);
+    const int jh = kSweepJH, wc = kSweepKW + 16 / (int)sizeof(T), w = kSweepKW;
     const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const int e = (int)sizeof(T);
     for (int c = 0; c < 3; c++) {
       if (int rc = make_map(&m.own[c], g.F[(esweep ? EX : HX) + c], dt, e, w, jh)) return rc;
-      if (int rc = make_map(&m.oth[c], g.F[(esweep ? HX : EX) + c], dt, e, w, jh + 1)) return rc;
+      if (int rc = make_map(&m.oth[c], g.F[(esweep ? HX : EX) + c], dt, e, wc, jh + 1)) return rc;
     }
     const int ncoef = esweep ? 6 : 3;
     for (int c = 0; c < ncoef; c++)
@@ -671,41 +677,124 @@ struct Engine : EngineBase {
       if (int rc = make_map(&m.idx, ci.idx, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, 32, jh)) return rc;
     if (has_pml) {
       const PmlFull<T> &pf = esweep ? pfe : pfh;
-      for (int c = 0; c < (esweep ? 6 : 3); c++)
+      for (int c = 0; c < (esweep ? 6 : 3); c++) {
         if (int rc = make_map(&m.aux[c], pf.aux[c], dt, e, w, jh)) return rc;
+        if (m.wn > 0)
+          if (int rc = make_map(&m.auxn[c], pf.aux[c], dt, e, m.wn, jh)) return rc;
+      }
     }
     return 0;
   }
 
-  // Tiles of kw (k) x 256/kw (j) columns over box u, i runs of ti planes.
-  static void add_sweep_tiles(std::vector<SweepTile> &out, int region, const Box &u, int ti, int kw)
+  static bool boxes_meet(const Box &u, const Box &v)
   {
-    if (u.empty()) return;
-    const int jh = 256 / kw;
-    const int kstart = kw == 32 ? (u.k0 / 32) * 32 : u.k0;
-    for (int i = u.i0; i <= u.i1; i += ti)
-      for (int j = u.j0; j <= u.j1; j += jh)
-        for (int k = kstart; k <= u.k1; k += kw)
-          out.push_back(SweepTile{ region, i, std::min(i + ti - 1, u.i1), j, k });
+    return !u.empty() && !v.empty() && u.i0 <= v.i1 && v.i0 <= u.i1 && u.j0 <= v.j1 && v.j0 <= u.j1 && u.k0 <= v.k1 &&
+           v.k0 <= u.k1;
   }
 
-  template <int KW, bool ES, bool PML>
+  static int64_t box_overlap(const Box &u, const Box &v)
+  {
+    if (!boxes_meet(u, v)) return 0;
+    Box x{ std::max(u.i0, v.i0), std::min(u.i1, v.i1), std::max(u.j0, v.j0),
+           std::min(u.j1, v.j1), std::max(u.k0, v.k0), std::min(u.k1, v.k1) };
+    return x.count();
+  }
+
+  static Box tile_box(const SweepTile &t)
+  {
+    return Box{ t.i0, t.i1, t.j0, t.j0 + kSweepJH - 1, t.k0, t.k0 + kSweepKW - 1 };
+  }
+
+  // Per-tile headers (see SweepHeader): membership masks, line lengths and
+  // UPML profiles, in the storage type, as the device arrays hold them.
+  template <bool ES, bool PML>
+  int build_headers(SweepLaunch &L, const std::vector<SweepTile> &tiles)
+  {
+    using Hdr = SweepHeader<T, PML>;
+    std::vector<Hdr> hv(tiles.size());
+    const Box *bb = ES ? be : bh;
+    const double *const *lines = ES ? p.idh : p.ide;
+    const double *const *prof[4] = { ES ? p.pml_ad : p.pml_ah, ES ? p.pml_bd : p.pml_bh, ES ? p.pml_ah : p.pml_ad,
+                                     ES ? p.pml_ibh : p.pml_ibd };
+    auto bits = [&](const SweepTile &t, int v, int axis) {
+      auto in = [&](const Box &b) {
+        const int lo = axis == 0 ? b.i0 : axis == 1 ? b.j0 : b.k0, hi = axis == 0 ? b.i1 : axis == 1 ? b.j1 : b.k1;
+        return (v >= lo && v <= hi) ? 1u : 0u;
+      };
+      uint32_t m = 0;
+      for (int c = 0; c < 3; c++) {
+        if (t.bulk) m |= in(bb[c]) << c;
+        if (PML && t.reg[0] >= 0) m |= in(pv.lim[t.reg[0]][(ES ? EX : HX) + c]) << (3 + c);
+        if (PML && t.reg[1] >= 0) m |= in(pv.lim[t.reg[1]][(ES ? EX : HX) + c]) << (6 + c);
+      }
+      return m;
+    };
+    auto at = [&](const double *a, int axis, int v) { return (a && v >= 0 && v < p.n[axis]) ? (T)a[v] : (T)0; };
+    for (size_t q = 0; q < tiles.size(); q++) {
+      const SweepTile &t = tiles[q];
+      Hdr &h = hv[q];
+      memset(&h, 0, sizeof h);
+      h.t = t;
+      const int n = t.i1 - t.i0 + 1;
+      for (int e = 0; e < kSweepMaxPlanes; e++) {
+        const int i = ES ? t.i0 + e : t.i1 - e;
+        h.plane_mask[e] = e < n ? bits(t, i, 0) : 0u;
+        h.dx[e] = at(lines[0], 0, i);
+        if (PML)
+          for (int a = 0; a < 4; a++) h.px[a][e] = at(prof[a][0], 0, i);
+      }
+      for (int r = 0; r < kSweepJH; r++) {
+        const int j = t.j0 + r;
+        h.row_mask[r] = j < p.n[1] ? bits(t, j, 1) : 0u;
+        h.dy[r] = at(lines[1], 1, j);
+        if (PML)
+          for (int a = 0; a < 4; a++) h.py[a][r] = at(prof[a][1], 1, j);
+      }
+      for (int c = 0; c < kSweepKW; c++) {
+        const int k = t.k0 + c;
+        h.col_mask[c] = bits(t, k, 2);
+        h.dz[c] = at(lines[2], 2, k);
+        if (PML)
+          for (int a = 0; a < 4; a++) h.pz[a][c] = at(prof[a][2], 2, k);
+      }
+    }
+    Hdr *d = nullptr;
+    if (upload(&d, hv.data(), hv.size())) return VGPU_ENOMEM;
+    L.headers = d;
+    return 0;
+  }
+
+  template <bool ES, bool PML>
   int prepare_launch(SweepLaunch &L, const std::vector<SweepTile> &tiles, bool compressed)
   {
     L.ntiles = (int)tiles.size();
     if (!L.ntiles) return 0;
+    for (const SweepTile &t : tiles)
+      if (t.i1 - t.i0 + 1 > kSweepMaxPlanes || t.k0 % kSweepKW)
+        return set_err(VGPU_EINVAL, "sweep tile of %d planes at k0=%d", t.i1 - t.i0 + 1, t.k0);
     if (upload(&L.tiles, tiles.data(), tiles.size())) return VGPU_ENOMEM;
-    L.smem = SweepLayout<T, KW, ES, PML>::smem_bytes(compressed);
-    auto kern = k_sweep_tma<T, KW, ES, PML>;
+    if (int rc = build_headers<ES, PML>(L, tiles)) return rc;
+    L.smem = SweepLayout<T, ES, PML>::smem_bytes(compressed);
+    auto kern = k_sweep_tma<T, ES, PML>;
     // The attribute is per kernel, shared by every engine in the process:
     // set it to the larger (uncompressed) layout.
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)SweepLayout<T, KW, ES, PML>::smem_bytes(false)));
+                            (int)SweepLayout<T, ES, PML>::smem_bytes(false)));
     int per_sm = 0, nsm = 148;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, L.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepThreads, L.smem));
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
     if (per_sm < 1) return set_err(VGPU_ECUDA, "sweep kernel does not fit on an SM (%u bytes of shared memory)", L.smem);
     L.grid = std::min(L.ntiles, per_sm * nsm);
+    // Points each launch updates, for throughput accounting.
+    const Box *bb = ES ? be : bh;
+    for (const SweepTile &t : tiles) {
+      const Box tb = tile_box(t);
+      for (int c = 0; c < 3; c++) {
+        if (t.bulk) L.bulk_points += box_overlap(tb, bb[c]);
+        for (int r = 0; r < 2; r++)
+          if (t.reg[r] >= 0) L.pml_points += box_overlap(tb, pv.lim[t.reg[r]][(ES ? EX : HX) + c]);
+      }
+    }
     return 0;
   }
 
@@ -741,96 +830,110 @@ struct Engine : EngineBase {
       CK(cudaMemset(aux, 0, sizeof(T) * vol * 9));
       for (int c = 0; c < 6; c++) pfe.aux[c] = aux + (int64_t)c * vol;
       for (int c = 0; c < 3; c++) pfh.aux[c] = aux + (int64_t)(6 + c) * vol;
-      for (PmlFull<T> *pf : { &pfe, &pfh }) {
-        for (int a = 0; a < 3; a++) {
-          pf->ad[a] = pv.ad[a]; pf->bd[a] = pv.bd[a]; pf->ah[a] = pv.ah[a];
-          pf->bh[a] = pv.bh[a]; pf->ibd[a] = pv.ibd[a]; pf->ibh[a] = pv.ibh[a];
-        }
-      }
-      for (int q = 0; q < pv.nreg; q++)
-        for (int c = 0; c < 3; c++) {
-          pfe.lim[q][c] = pv.lim[q][EX + c];
-          pfh.lim[q][c] = pv.lim[q][HX + c];
-        }
     }
-    // Tiles: i runs sized so each launch has several tiles per resident
-    // block, for balance; the pipeline runs across tile boundaries.
+    // Tiles: 32 x 8 columns, i runs sized so each launch has several tiles
+    // per resident block, for balance; the pipeline runs across tile
+    // boundaries.  Bulk-footprint tiles whose rows reach into a Z region
+    // (the thin UPML slabs at the k ends) go to the UPML kernel with both
+    // the bulk box and the Z region boxes; the X and Y regions get their own
+    // tiles.
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
     auto run_len = [&](int64_t cells) {
       int64_t t = cells / (256LL * nsm * 16);
-      return (int)std::max<int64_t>(4, std::min<int64_t>(32, t));
+      return (int)std::max<int64_t>(4, std::min<int64_t>(kSweepMaxPlanes, t));
     };
+    const int halo = 16 / (int)sizeof(T);
     for (int es = 0; es < 2; es++) {
       const Box &ub = es ? ube : ubh;
-      std::vector<SweepTile> bulk, p32, p8;
-      add_sweep_tiles(bulk, -1, ub, run_len(ub.count()), 32);
+      std::vector<SweepTile> bulk, pml;
+      int wn = 0;
+      Box zun[2];
+      int zreg[2] = { -1, -1 }, nz = 0;
+      Box core = ub;
       for (int q = 0; q < pv.nreg; q++) {
         Box c3[3] = { pv.lim[q][es ? EX : HX], pv.lim[q][es ? EY : HY], pv.lim[q][es ? EZ : HZ] };
         Box u = unite(c3);
         if (u.i1 < u.i0) continue;
-        if (pml_face[q] / 2 == 2)
-          add_sweep_tiles(p8, q, u, run_len(u.count()), 8);
-        else
-          add_sweep_tiles(p32, q, u, run_len(u.count()), 32);
+        if (pml_face[q] / 2 == 2) {
+          zun[nz] = u;
+          zreg[nz++] = q;
+          if (core.empty()) core = u;
+          core = Box{ std::min(core.i0, u.i0), std::max(core.i1, u.i1), std::min(core.j0, u.j0),
+                      std::max(core.j1, u.j1), std::min(core.k0, u.k0), std::max(core.k1, u.k1) };
+        } else {
+          const int ti = run_len(u.count());
+          for (int i = u.i0; i <= u.i1; i += ti)
+            for (int j = u.j0; j <= u.j1; j += kSweepJH)
+              for (int k = (u.k0 / kSweepKW) * kSweepKW; k <= u.k1; k += kSweepKW)
+                pml.push_back(SweepTile{ { q, -1 }, 0, i, std::min(i + ti - 1, u.i1), j, k, -1 });
+        }
       }
+      if (!core.empty()) {
+        const int ti = run_len(core.count());
+        for (int i = core.i0; i <= core.i1; i += ti)
+          for (int j = core.j0; j <= core.j1; j += kSweepJH)
+            for (int k = (core.k0 / kSweepKW) * kSweepKW; k <= core.k1; k += kSweepKW) {
+              SweepTile t{ { -1, -1 }, 1, i, std::min(i + ti - 1, core.i1), j, k, -1 };
+              const Box tb = tile_box(t);
+              int r = 0, zi = -1;
+              for (int z = 0; z < nz; z++)
+                if (boxes_meet(tb, zun[z])) {
+                  t.reg[r++] = zreg[z];
+                  zi = z;
+                }
+              // One Z slab: its auxiliaries in a narrow box over its columns.
+              if (r == 1) {
+                const int ax = std::max(zun[zi].k0, k) & ~(halo - 1);
+                t.ax = ax;
+                wn = std::max(wn, std::min(zun[zi].k1, k + kSweepKW - 1) - ax + 1);
+              }
+              (r ? pml : bulk).push_back(t);
+            }
+      }
+      // Narrow boxes must stay narrower than the full ones; else use those.
+      wn = (wn + halo - 1) / halo * halo;
+      if (wn > kSweepKW)
+        for (SweepTile &t : pml) t.ax = -1;
+      (es ? maps_e : maps_h).wn = wn > kSweepKW ? 0 : wn;
       SweepLaunch *L = es ? sw_e : sw_h;
-      bool comp = (es ? cie : cih).idx != nullptr;
+      const bool comp = (es ? cie : cih).idx != nullptr;
       if (es) {
-        if (int rc = prepare_launch<32, true, false>(L[0], bulk, comp)) return rc;
-        if (int rc = prepare_launch<32, true, true>(L[1], p32, comp)) return rc;
-        if (int rc = prepare_launch<8, true, true>(L[2], p8, comp)) return rc;
+        if (int rc = prepare_launch<true, false>(L[0], bulk, comp)) return rc;
+        if (int rc = prepare_launch<true, true>(L[1], pml, comp)) return rc;
       } else {
-        if (int rc = prepare_launch<32, false, false>(L[0], bulk, comp)) return rc;
-        if (int rc = prepare_launch<32, false, true>(L[1], p32, comp)) return rc;
-        if (int rc = prepare_launch<8, false, true>(L[2], p8, comp)) return rc;
+        if (int rc = prepare_launch<false, false>(L[0], bulk, comp)) return rc;
+        if (int rc = prepare_launch<false, true>(L[1], pml, comp)) return rc;
       }
     }
-    if (int rc = make_sweep_maps(maps_e32, true, 32)) return rc;
-    if (int rc = make_sweep_maps(maps_h32, false, 32)) return rc;
-    if (int rc = make_sweep_maps(maps_e8, true, 8)) return rc;
-    if (int rc = make_sweep_maps(maps_h8, false, 8)) return rc;
+    if (int rc = make_sweep_maps(maps_e, true)) return rc;
+    if (int rc = make_sweep_maps(maps_h, false)) return rc;
     return 0;
   }
 
-  // Launch the sweeps of one half step: which = 0 bulk, 1 PML (both row
-  // widths).  Returns the number of kernels launched through `count`.
+  // Launch one sweep kernel of a half step: which = 0 the bulk tiles, 1 the
+  // UPML and mixed tiles.  Counts launched kernels through `count`.
   int launch_sweeps(bool esweep, int which, uint64_t *count)
   {
-    const dim3 blk(256);
-    SweepLaunch *L = esweep ? sw_e : sw_h;
-    const Box *bb = esweep ? be : bh;
+    const dim3 blk(kSweepThreads);
+    SweepLaunch &L = (esweep ? sw_e : sw_h)[which];
+    if (!L.ntiles) return 0;
     const CoefIndex &ci = esweep ? cie : cih;
     const PmlFull<T> &pf = esweep ? pfe : pfh;
-    if (which == 0 && L[0].ntiles) {
-      if (esweep)
-        k_sweep_tma<T, 32, true, false><<<L[0].grid, blk, L[0].smem, s>>>(maps_e32, g, L[0].tiles, L[0].ntiles, bb[0],
-                                                                          bb[1], bb[2], pf, ci, d_err);
-      else
-        k_sweep_tma<T, 32, false, false><<<L[0].grid, blk, L[0].smem, s>>>(maps_h32, g, L[0].tiles, L[0].ntiles, bb[0],
-                                                                           bb[1], bb[2], pf, ci, d_err);
-      if (count) ++*count;
-    }
-    if (which == 1) {
-      if (L[1].ntiles) {
-        if (esweep)
-          k_sweep_tma<T, 32, true, true><<<L[1].grid, blk, L[1].smem, s>>>(maps_e32, g, L[1].tiles, L[1].ntiles, bb[0],
-                                                                           bb[1], bb[2], pf, ci, d_err);
-        else
-          k_sweep_tma<T, 32, false, true><<<L[1].grid, blk, L[1].smem, s>>>(maps_h32, g, L[1].tiles, L[1].ntiles, bb[0],
-                                                                            bb[1], bb[2], pf, ci, d_err);
-        if (count) ++*count;
-      }
-      if (L[2].ntiles) {
-        if (esweep)
-          k_sweep_tma<T, 8, true, true><<<L[2].grid, blk, L[2].smem, s>>>(maps_e8, g, L[2].tiles, L[2].ntiles, bb[0],
-                                                                          bb[1], bb[2], pf, ci, d_err);
-        else
-          k_sweep_tma<T, 8, false, true><<<L[2].grid, blk, L[2].smem, s>>>(maps_h8, g, L[2].tiles, L[2].ntiles, bb[0],
-                                                                           bb[1], bb[2], pf, ci, d_err);
-        if (count) ++*count;
-      }
-    }
+    const SweepMaps &mp = esweep ? maps_e : maps_h;
+    if (esweep && which == 0)
+      k_sweep_tma<T, true, false><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
+                                                            L.ntiles, pf, ci, d_err);
+    else if (esweep)
+      k_sweep_tma<T, true, true><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
+                                                           L.ntiles, pf, ci, d_err);
+    else if (which == 0)
+      k_sweep_tma<T, false, false><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
+                                                             L.ntiles, pf, ci, d_err);
+    else
+      k_sweep_tma<T, false, true><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
+                                                            L.ntiles, pf, ci, d_err);
+    if (count) ++*count;
     return 0;
   }
 
@@ -1139,7 +1242,7 @@ struct Engine : EngineBase {
     const bool es = kernel == VGPU_K_BULK_E || kernel == VGPU_K_PML_E;
     const int which = (kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) ? 0 : 1;
     const SweepLaunch *L = es ? sw_e : sw_h;
-    const bool present = which == 0 ? L[0].ntiles > 0 : (L[1].ntiles + L[2].ntiles) > 0;
+    const bool present = L[which].ntiles > 0;
     if (kernel < 0 || kernel > 3 || !present) {
       if (!required) return 0;
       return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
@@ -1147,15 +1250,21 @@ struct Engine : EngineBase {
     return launch_sweeps(es, which, count);
   }
 
+  int sweep_points(int kernel, uint64_t *bulk_pts, uint64_t *pml_pts) override
+  {
+    if (kernel < 0 || kernel > 3) return set_err(VGPU_EINVAL, "kernel %d is not a sweep", kernel);
+    const bool es = kernel == VGPU_K_BULK_E || kernel == VGPU_K_PML_E;
+    const SweepLaunch &L = (es ? sw_e : sw_h)[(kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) ? 0 : 1];
+    *bulk_pts = L.bulk_points;
+    *pml_pts = L.pml_points;
+    return 0;
+  }
+
   int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override
   {
-    uint64_t pts = 0;
-    if (kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) {
-      for (int c = 0; c < 3; c++) pts += (kernel == VGPU_K_BULK_H ? bh : be)[c].count();
-    }
-    else if (kernel == VGPU_K_PML_E || kernel == VGPU_K_PML_H)
-      for (int r = 0; r < pv.nreg; r++)
-        for (int c = 0; c < 3; c++) pts += pv.lim[r][kernel == VGPU_K_PML_E ? c : 3 + c].count();
+    uint64_t bulk_pts = 0, pml_pts = 0;
+    if (int rc = sweep_points(kernel, &bulk_pts, &pml_pts)) return rc;
+    const uint64_t pts = bulk_pts + pml_pts;
     for (int q = 0; q < warmup; q++)
       if (int rc = launch_one(kernel)) return rc;
     cudaEvent_t e0, e1;
@@ -1307,6 +1416,12 @@ extern "C" int vgpu_check_finite(vgpu_engine *e)
 }
 
 extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
+
+extern "C" int vgpu_sweep_points(const vgpu_engine *e, int32_t kernel, uint64_t *bulk_points, uint64_t *pml_points)
+{
+  if (!e || !bulk_points || !pml_points) return set_err(VGPU_EINVAL, "null argument");
+  return e->impl->sweep_points(kernel, bulk_points, pml_points);
+}
 
 extern "C" int vgpu_set_bin_sink(vgpu_engine *e, vgpu_bin_sink sink, void *user)
 {

@@ -1,20 +1,29 @@
 // sweep_tma.cuh -- TMA-pipelined E and H sweeps (sm_100a).
 //
 // The bulk Yee updates (src/grid.c:709-888) and the UPML updates
-// (src/pml.c:859-1176) as persistent marching sweeps.  The host cuts each
-// update region into tiles of KW (k) x JH (j) columns and a run of i planes
-// (JH = 256 / KW); a block owns a strided subset of the tiles and walks
-// their planes in order.  One thread per (j,k) column.
+// (src/pml.c:859-1176) as persistent marching sweeps.  The host cuts the
+// grid into tiles of 32 (k) x 8 (j) columns and a run of i planes; a block
+// owns a strided subset of the tiles and walks their planes in order.
+// Eight compute warps hold one (j,k) column per thread; lane 0 of a ninth
+// warp issues the loads.
 //
 // Data movement: every plane a tile needs is brought into shared memory by
 // cp.async.bulk.tensor (TMA) loads -- the updated component boxes, the
-// curl's component boxes with a one-row / one-column halo, the coefficient
-// index (or the coefficient volumes), and for UPML tiles the auxiliary
-// fields -- into a ring of S stages, each with an mbarrier that completes
-// when its bytes have landed.  Thread 0 keeps the ring full across tile
-// boundaries, so the loads of the next S-2 planes are in flight while a
-// plane is computed.  Stores go straight to global memory, predicated on the
-// component's update box, one coalesced row per warp.
+// curl's component boxes with a one-row / 16-byte halo, the coefficient
+// index (or the coefficient volumes), and for tiles with UPML points the
+// auxiliary fields -- into a ring of S stages.  Each stage has an mbarrier
+// that completes when its bytes have landed and a second one that completes
+// when the compute warps have read it.  The producer keeps the ring full
+// across tile boundaries, so the next planes' loads are in flight while a
+// plane is computed.  Stores go straight to global memory, predicated on
+// the point's update box, one coalesced row per warp.
+//
+// Two kernels per half step.  The bulk kernel takes tiles that hold only
+// bulk points.  The UPML kernel takes the X and Y regions' tiles and the
+// bulk-footprint tiles whose k rows reach into a Z region; each point picks
+// the bulk or the UPML update from the boxes it lies in, so the thin Z
+// slabs ride in the same 32-wide rows as the bulk next to them, with their
+// auxiliaries in narrow boxes over the slab's columns.
 //
 // Plane bookkeeping: a tile with planes i0..i1 (n planes) uses n + 1
 // stages.  The E sweep marches up: stage 0 holds only Hy, Hz of plane
@@ -22,13 +31,14 @@
 // i0 - 1 + q.  The H sweep marches down: stage 0 holds only Ey, Ez of plane
 // i1 + 1 and stage q >= 1 plane i1 + 1 - q.  Plane p of the march reads
 // stage p + 1; the neighbour plane's two values come from stage 0 for
-// p = 0 and from the previous plane (kept in registers) after that.  Every
-// thread waits on the stages it reads; a block-wide vote then releases the
-// stages before it to the producer, so three stages suffice.
+// p = 0 and from the previous plane (kept in registers) after that.
+// Stage 0 also brings the tile's header (SweepHeader), built on the host,
+// so the compute warps read nothing from global memory.
 //
 // Every mbarrier wait is bounded.  A wait that runs out records an error
-// code in *err, waits (bounded) for the loads the block still has in
-// flight, and leaves the block; the host reports VGPU_ETIMEOUT.
+// code in *err and ends the warp; the producer, the block's last thread,
+// first waits (bounded) for the loads it has in flight.  The host reports
+// VGPU_ETIMEOUT, and later launches of the run return at once.
 //
 // UPML auxiliaries live in full-volume arrays indexed like the fields.  The
 // update regions of one component never overlap (the engine checks this at
@@ -43,7 +53,7 @@
 namespace vgpu_dev {
 
 // Bound on mbarrier polls; each poll may suspend for up to the hint below,
-// so a lost transfer ends the block after about a second.
+// so a lost transfer ends the warp after about a second.
 constexpr uint32_t kSpinLimit = 1u << 20;
 constexpr uint32_t kSuspendHintNs = 1000;
 
@@ -94,43 +104,95 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
-// Tensor maps of one sweep and tile shape.  own: the three updated
-// components, box (W, JH); oth: the curl's three components, box (W, JH+1);
-// coef: alpha/beta (E) or gamma (H) volumes, box (W, JH); idx: the one-byte
-// coefficient index, box (32 bytes, JH); aux: PP0..2, P0..2 (E) or B0..2 (H).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global to shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Tensor maps of one sweep.  own: the three updated components, box
+// (32, 8); oth: the curl's three components, box (32 + halo, 9); coef:
+// alpha/beta (E) or gamma (H) volumes, box (32, 8); idx: the one-byte
+// coefficient index, box (32 bytes, 8); aux: PP0..2, P0..2 (E) or B0..2
+// (H), box (32, 8); auxn: the same volumes, box (wn, 8), over a Z slab's
+// columns only.
 struct SweepMaps {
   CUtensorMap own[3];
   CUtensorMap oth[3];
   CUtensorMap coef[6];
   CUtensorMap idx;
   CUtensorMap aux[6];
+  CUtensorMap auxn[6];
+  int wn;              // width of the auxn boxes in elements (0: unused)
 };
 
-// Full-volume UPML state and 1-D profiles for the sweeps.
+// Full-volume UPML auxiliaries of one sweep.
 template <typename T>
 struct PmlFull {
-  const T *ad[3], *bd[3], *ah[3], *bh[3], *ibd[3], *ibh[3];
   T *aux[6];           // PP0..2, P0..2 (E sweep) or B0..2 (H sweep)
-  Box lim[6][3];       // [region][component of this sweep]
 };
 
+// A tile: planes i0..i1 of the 32 x 8 columns starting at (j0, k0), k0 a
+// multiple of 32.  Its points update with the bulk formula where `bulk` is
+// set and they lie in the bulk box, and with the UPML formula where they lie
+// in the box of region reg[0] or reg[1] (-1: none).  UPML auxiliaries come
+// in full-width boxes (ax < 0) or, for a tile whose only UPML points are
+// one Z slab, in narrow boxes starting at column ax.
 struct SweepTile {
-  int region;          // -1 bulk, else PML region ordinal
-  int i0, i1;          // planes (inclusive)
-  int j0, k0;          // first column
+  int reg[2];
+  int bulk;
+  int i0, i1;
+  int j0, k0;
+  int ax;
+};
+
+constexpr int kSweepKW = 32;   // k columns per tile (one warp row)
+constexpr int kSweepJH = 8;    // j rows per tile (one per compute warp)
+constexpr int kSweepMaxPlanes = 32;
+constexpr int kSweepThreads = 288;
+
+// Per-tile values, built on the host and copied into shared memory with the
+// tile's stage 0: the tile, per-plane line lengths and UPML x profiles
+// (entry p = plane p of the march), per-row and per-column ones, and
+// box-membership masks (bit c: bulk box of component c, bit 3+c: region
+// reg[0], bit 6+c: region reg[1]); a point's mask is
+// row_mask[j] & col_mask[k] & plane_mask[p].  UPML profiles are ordered
+// (a, b, c, d) = (ad, bd, ah, ibh) for E and (ah, bh, ad, ibd) for H.
+template <typename T, bool PML>
+struct alignas(16) SweepHeader {
+  SweepTile t;
+  uint32_t plane_mask[kSweepMaxPlanes];
+  uint32_t row_mask[kSweepJH];
+  uint32_t col_mask[kSweepKW];
+  T dx[kSweepMaxPlanes];
+  T dy[kSweepJH];
+  T dz[kSweepKW];
+  T px[PML ? 4 : 1][kSweepMaxPlanes];
+  T py[PML ? 4 : 1][kSweepJH];
+  T pz[PML ? 4 : 1][kSweepKW];
 };
 
 __host__ __device__ constexpr uint32_t round128(uint32_t b) { return (b + 127u) / 128u * 128u; }
 
-template <typename T, int KW, bool ESWEEP, bool PML>
+template <typename T, bool ESWEEP, bool PML>
 struct SweepLayout {
-  static constexpr int JH = 256 / KW;
+  static constexpr int JH = kSweepJH;
   static constexpr int HALO = 16 / (int)sizeof(T);   // elements per 16 bytes
-  static constexpr int W = KW + HALO;                // box width in elements
+  static constexpr int W = kSweepKW + HALO;          // curl boxes: the tile row plus a halo
   static constexpr int NCOEF = ESWEEP ? 6 : 3;
   static constexpr int NAUX = PML ? (ESWEEP ? 6 : 3) : 0;
-  static constexpr int S = (sizeof(T) == 8 && PML) ? 3 : 4;   // >= 3 (see above)
-  static constexpr uint32_t OWN_B = (uint32_t)(W * JH * sizeof(T));
+  static constexpr int S = (sizeof(T) == 8 && PML) ? 3 : 4;   // ring depth
+  static constexpr int MIN_BLOCKS = sizeof(T) == 4 ? (PML ? 3 : 4) : 2;
+  static constexpr uint32_t OWN_B = (uint32_t)(kSweepKW * JH * sizeof(T));
   static constexpr uint32_t OTH_B = (uint32_t)(W * (JH + 1) * sizeof(T));
   static constexpr uint32_t IDX_B = 32u * JH;
   static constexpr uint32_t OFF_OWN = 0;
@@ -141,142 +203,174 @@ struct SweepLayout {
   {
     return OFF_CF + (compressed ? round128(IDX_B) : NCOEF * round128(OWN_B));
   }
-  // Bytes a full stage receives, and a partial one (two curl components).
+  // Bytes a full stage receives, with full-width auxiliaries.
   __host__ __device__ static constexpr uint32_t full_tx(bool compressed)
   {
     return 3 * OWN_B + 3 * OTH_B + NAUX * OWN_B + (compressed ? IDX_B : NCOEF * OWN_B);
   }
-  static constexpr uint32_t PARTIAL_TX = 2 * OTH_B;
+  // Stage 0: two curl components and the header.
+  static constexpr uint32_t PARTIAL_TX = 2 * OTH_B + (uint32_t)sizeof(SweepHeader<T, PML>);
   __host__ __device__ static constexpr uint32_t smem_bytes(bool compressed) { return S * stage_bytes(compressed); }
 };
 
-template <typename T, int KW, bool ESWEEP, bool PML>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && !PML) ? 4 : 2)
-    k_sweep_tma(const __grid_constant__ SweepMaps maps, Grid<T> g, const SweepTile *__restrict__ tiles, int ntiles,
-                Box b0in, Box b1in, Box b2in, PmlFull<T> pf, CoefIndex ci, int *err)
+// Block: warps 0..7 compute, warp 8 lane 0 produces.
+template <typename T, bool ESWEEP, bool PML>
+__global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MIN_BLOCKS)
+    k_sweep_tma(const __grid_constant__ SweepMaps maps, Grid<T> g, const SweepTile *__restrict__ tiles,
+                const SweepHeader<T, PML> *__restrict__ headers, int ntiles, PmlFull<T> pf, CoefIndex ci, int *err)
 {
-  using L = SweepLayout<T, KW, ESWEEP, PML>;
-  constexpr int S = L::S, W = L::W, HALO = L::HALO;
+  using L = SweepLayout<T, ESWEEP, PML>;
+  using Hdr = SweepHeader<T, PML>;
+  constexpr int S = L::S, W = L::W, HALO = L::HALO, KW = kSweepKW;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t full[S];
+  __shared__ uint64_t full[S], empty[S];
   __shared__ T tab[256 * L::NCOEF];
+  __shared__ Hdr hdr[2];
   __shared__ int sh_err;
 
   const bool compressed = ci.idx != nullptr;
   const uint32_t stage_b = L::stage_bytes(compressed);
-  const uint32_t full_tx = L::full_tx(compressed);
   const int tid = threadIdx.x;
-  const int kl = tid % KW, jl = tid / KW;
+  const int warp = tid / 32, lane = tid % 32;
 
   if (tid == 0) {
     // After an earlier pipeline failure the run is lost: skip the work.
     sh_err = *(volatile int *)err;
-    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    for (int s = 0; s < S; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 8);
+    }
     mbar_fence_init();
   }
   if (compressed) {
     const T *src = (const T *)ci.table;
-    for (int q = tid; q < ci.ntab * L::NCOEF; q += 256) tab[q] = src[q];
+    for (int q = tid; q < ci.ntab * L::NCOEF; q += kSweepThreads) tab[q] = src[q];
   }
   __syncthreads();
   if (sh_err) return;
 
-  // Producer cursor (thread 0): next tile ordinal and stage within it.
-  int pm = 0, pq = 0;
-  int64_t issued = 0, waited = 0;
-
-  auto produce_one = [&]() -> bool {
-    const int tile_id = blockIdx.x + pm * gridDim.x;
-    if (tile_id >= ntiles) return false;
-    const SweepTile tt = tiles[tile_id];
-    const int n = tt.i1 - tt.i0 + 1;
-    const int slot = (int)(issued % S);
-    unsigned char *st = smem + (size_t)slot * stage_b;
-    uint64_t *bar = &full[slot];
-    const int xs_e = tt.k0 & ~(HALO - 1);
-    const int xs_o = ESWEEP ? ((tt.k0 - 1) & ~(HALO - 1)) : xs_e;
-    const int yo = ESWEEP ? tt.j0 - 1 : tt.j0;
-    const int i = ESWEEP ? tt.i0 - 1 + pq : tt.i1 + 1 - pq;
-    const bool partial = pq == 0;
-    if (partial) {
-      mbar_arrive_expect_tx(bar, L::PARTIAL_TX);
-      for (int c = 1; c < 3; c++) tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
-    } else {
-      mbar_arrive_expect_tx(bar, full_tx);
-      for (int c = 0; c < 3; c++) tma_load_3d(st + L::OFF_OWN + c * round128(L::OWN_B), &maps.own[c], bar, xs_e, tt.j0, i);
-      for (int c = 0; c < 3; c++) tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
-      for (int c = 0; c < L::NAUX; c++)
-        tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.aux[c], bar, xs_e, tt.j0, i);
-      if (compressed)
-        tma_load_3d(st + L::OFF_CF, &maps.idx, bar, tt.k0 & ~15, tt.j0, i);
-      else
-        for (int c = 0; c < L::NCOEF; c++)
-          tma_load_3d(st + L::OFF_CF + c * round128(L::OWN_B), &maps.coef[c], bar, xs_e, tt.j0, i);
+  if (warp == 8) {
+    // ---- producer ----
+    if (lane != 0) return;
+    const uint32_t full_tx = L::full_tx(compressed);
+    const uint32_t narrow_tx = full_tx - L::NAUX * L::OWN_B + L::NAUX * (uint32_t)(maps.wn * L::JH * sizeof(T));
+    uint32_t gs = 0;
+    bool ok = true;
+    int id = blockIdx.x;
+    SweepTile tt = id < ntiles ? tiles[id] : SweepTile{};
+    for (uint32_t m = 0; ok && id < ntiles; m++) {
+      // The next tile's record loads while this one issues.
+      const int id_next = id + (int)gridDim.x;
+      const SweepTile nt = id_next < ntiles ? tiles[id_next] : SweepTile{};
+      const int n = tt.i1 - tt.i0 + 1;
+      const int xs_o = ESWEEP ? tt.k0 - HALO : tt.k0;
+      const int yo = ESWEEP ? tt.j0 - 1 : tt.j0;
+      for (int q = 0; q <= n; q++) {
+        const uint32_t slot = gs % S;
+        if (gs >= S && !mbar_wait(&empty[slot], ((gs / S) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        unsigned char *st = smem + slot * stage_b;
+        uint64_t *bar = &full[slot];
+        const int i = ESWEEP ? tt.i0 - 1 + q : tt.i1 + 1 - q;
+        if (q == 0) {
+          mbar_arrive_expect_tx(bar, L::PARTIAL_TX);
+          bulk_load(&hdr[m & 1], headers + id, (uint32_t)sizeof(Hdr), bar);
+          for (int c = 1; c < 3; c++)
+            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
+        } else {
+          mbar_arrive_expect_tx(bar, tt.ax < 0 ? full_tx : narrow_tx);
+          for (int c = 0; c < 3; c++)
+            tma_load_3d(st + L::OFF_OWN + c * round128(L::OWN_B), &maps.own[c], bar, tt.k0, tt.j0, i);
+          for (int c = 0; c < 3; c++)
+            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
+          for (int c = 0; c < L::NAUX; c++) {
+            if (tt.ax < 0)
+              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.aux[c], bar, tt.k0, tt.j0, i);
+            else
+              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.auxn[c], bar, tt.ax, tt.j0, i);
+          }
+          if (compressed)
+            tma_load_3d(st + L::OFF_CF, &maps.idx, bar, tt.k0, tt.j0, i);
+          else
+            for (int c = 0; c < L::NCOEF; c++)
+              tma_load_3d(st + L::OFF_CF + c * round128(L::OWN_B), &maps.coef[c], bar, tt.k0, tt.j0, i);
+        }
+        gs++;
+      }
+      id = id_next;
+      tt = nt;
     }
-    issued++;
-    if (++pq > n) { pq = 0; pm++; }
-    return true;
-  };
+    if (!ok) atomicCAS(err, 0, 1);
+    // No load may still be in flight when the block's last thread leaves.
+    for (uint32_t q = gs > S ? gs - S : 0; q < gs; q++) (void)mbar_wait(&full[q % S], (q / S) & 1);
+    return;
+  }
 
-  if (tid == 0)
-    while (issued < S && produce_one()) {}
-
+  // ---- compute warps ----
+  const int kl = tid % KW, jl = tid / KW;
   T *__restrict__ F0 = g.F[ESWEEP ? EX : HX];
   T *__restrict__ F1 = g.F[ESWEEP ? EY : HY];
   T *__restrict__ F2 = g.F[ESWEEP ? EZ : HZ];
-
-  int64_t cg = 0;  // stage index of the current tile's stage 0
-  bool failed = false;
-  for (int m = 0; !failed; m++) {
-    const int tile_id = blockIdx.x + m * gridDim.x;
-    if (tile_id >= ntiles) break;
-    const SweepTile t = tiles[tile_id];
-    const int n = t.i1 - t.i0 + 1;
-    Box b0 = b0in, b1 = b1in, b2 = b2in;
-    if (PML) {
-      b0 = pf.lim[t.region][0];
-      b1 = pf.lim[t.region][1];
-      b2 = pf.lim[t.region][2];
+  const int io = jl * KW + kl;                        // row-wide boxes
+  const int ih = (ESWEEP ? jl + 1 : jl) * W + (ESWEEP ? kl + HALO : kl);   // curl boxes
+  uint32_t gs = 0;
+  for (uint32_t m = 0;; m++) {
+    if ((int)(blockIdx.x + m * gridDim.x) >= ntiles) return;
+    // Stage 0 of the tile, with its header.
+    uint32_t slot = gs % S;
+    bool ok = mbar_wait(&full[slot], (gs / S) & 1);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicCAS(err, 0, 1);
+      return;
     }
+    const Hdr &h = hdr[m & 1];
+    const SweepTile t = h.t;
+    const int n = t.i1 - t.i0 + 1;
     const int k = t.k0 + kl;
     const int j = t.j0 + jl;
-    const bool jok = j < g.n1;
-    const int xs_e = t.k0 & ~(HALO - 1);
-    const int xs_o = ESWEEP ? ((t.k0 - 1) & ~(HALO - 1)) : xs_e;
-    const int io = jl * W + (k - xs_e);                        // own boxes
-    const int ih = (ESWEEP ? jl + 1 : jl) * W + (k - xs_o);    // curl boxes
-    const int ii = jl * 32 + (k - (t.k0 & ~15));              // index box
-    const int jc = jok ? j : g.n1 - 1;
+    // UPML auxiliaries: full-width boxes share the row-wide layout.
+    const int ia = t.ax < 0 ? io : jl * maps.wn + (k - t.ax);
+    const int jc = min(j, g.n1 - 1);
     const int kc = min(k, (int)g.s1 - 1);
-    const T d1 = ld((ESWEEP ? g.idh[1] : g.ide[1]) + jc);
-    const T d2 = ld((ESWEEP ? g.idh[2] : g.ide[2]) + kc);
-    // The neighbour plane's two curl components at this column: Hy, Hz of
-    // plane i-1 (E sweep) or Ey, Ez of plane i+1 (H sweep).
-    T nb1 = 0, nb2 = 0;
+    const int64_t x0 = (int64_t)jc * g.s1 + kc;
+    const uint32_t col = h.row_mask[jl] & h.col_mask[kl];
+    const uint32_t pm_l = h.plane_mask[lane];
+    const T d1 = h.dy[jl], d2 = h.dz[kl], dx_l = h.dx[lane];
+    T pa_l = 0, pb_l = 0, pc_l = 0, pd_l = 0;   // x profiles of plane = lane
+    T q1a = 0, q1b = 0, q1c = 0, q1d = 0;       // y profiles of this row
+    T q2a = 0, q2b = 0, q2c = 0, q2d = 0;       // z profiles of this column
+    if (PML) {
+      pa_l = h.px[0][lane]; pb_l = h.px[1][lane]; pc_l = h.px[2][lane]; pd_l = h.px[3][lane];
+      q1a = h.py[0][jl]; q1b = h.py[1][jl]; q1c = h.py[2][jl]; q1d = h.py[3][jl];
+      q2a = h.pz[0][kl]; q2b = h.pz[1][kl]; q2c = h.pz[2][kl]; q2d = h.pz[3][kl];
+    }
+    // The neighbour plane's two curl components at this column -- Hy, Hz of
+    // plane i0-1 (E sweep) or Ey, Ez of plane i1+1 (H sweep).
+    T nb1, nb2;
+    {
+      const unsigned char *st = smem + slot * stage_b;
+      nb1 = ((const T *)(st + L::OFF_OTH + round128(L::OTH_B)))[ih];
+      nb2 = ((const T *)(st + L::OFF_OTH + 2 * round128(L::OTH_B)))[ih];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[slot]);
+      gs++;
+    }
 
     for (int p = 0; p < n; p++) {
-      const int64_t A = cg + p + 1;
-      bool ok = true;
-      if (p == 0) {
-        ok = mbar_wait(&full[cg % S], (uint32_t)((cg / S) & 1));
-        if (ok) {
-          const unsigned char *s0p = smem + (size_t)(cg % S) * stage_b;
-          nb1 = ((const T *)(s0p + L::OFF_OTH + round128(L::OTH_B)))[ih];
-          nb2 = ((const T *)(s0p + L::OFF_OTH + 2 * round128(L::OTH_B)))[ih];
-        }
+      slot = gs % S;
+      ok = mbar_wait(&full[slot], (gs / S) & 1);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicCAS(err, 0, 1);
+        return;
       }
-      if (ok) ok = mbar_wait(&full[A % S], (uint32_t)((A / S) & 1));
-      if (tid == 0 && ok) waited = A + 1;
-      // Uniform decision, and every thread is done with the stages before A.
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        break;
-      }
-      if (tid == 0)
-        while (issued < A + S && produce_one()) {}
-
       const int i = ESWEEP ? t.i0 + p : t.i1 - p;
-      const unsigned char *sc = smem + (size_t)(A % S) * stage_b;
+      const T dx = __shfl_sync(0xffffffffu, dx_l, p);
+      const uint32_t m9 = col & __shfl_sync(0xffffffffu, pm_l, p);
+      // Which update each component takes: bit c bulk, bit 3+c UPML.
+      const uint32_t sel = (m9 & 7u) | ((m9 | (m9 >> 3)) & 56u);
+      const unsigned char *sc = smem + slot * stage_b;
       const T *own0 = (const T *)(sc + L::OFF_OWN);
       const T *own1 = (const T *)(sc + L::OFF_OWN + round128(L::OWN_B));
       const T *own2 = (const T *)(sc + L::OFF_OWN + 2 * round128(L::OWN_B));
@@ -287,7 +381,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !PML) ? 4 : 2)
       T cf[L::NCOEF];
       if (compressed) {
         const uint8_t *ix = (const uint8_t *)(sc + L::OFF_CF);
-        const T *cw = tab + L::NCOEF * (int)ix[ii];
+        const T *cw = tab + L::NCOEF * (int)ix[io];
 #pragma unroll
         for (int c = 0; c < L::NCOEF; c++) cf[c] = cw[c];
       } else {
@@ -295,109 +389,103 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !PML) ? 4 : 2)
         for (int c = 0; c < L::NCOEF; c++) cf[c] = ((const T *)(sc + L::OFF_CF + c * round128(L::OWN_B)))[io];
       }
       const T v0 = own0[io], v1 = own1[io], v2 = own2[io];
-      const bool s0 = jok && b0.contains(i, j, k);
-      const bool s1 = jok && b1.contains(i, j, k);
-      const bool s2 = jok && b2.contains(i, j, k);
-      const int64_t x = g.at(i, jc, kc);
       T c0, c1, c2;
       if (ESWEEP) {
-        // curl H (src/grid.h:139-167): hz_jm = Hz(j-1), hy_km = Hy(k-1),
-        // hx_km = Hx(k-1), hx_jm = Hx(j-1); nb = H of plane i-1.
-        const T idhx = ld(g.idh[0] + i);
+        // curl H (src/grid.h:139-167): Hz(j-1), Hy(k-1), Hx(k-1), Hx(j-1),
+        // and the i-1 plane's Hy, Hz from the previous plane.
         const T hx = oth0[ih], hy = oth1[ih], hz = oth2[ih];
         c0 = d1 * (hz - oth2[ih - W]) + d2 * (oth1[ih - 1] - hy);
-        c1 = d2 * (hx - oth0[ih - 1]) + idhx * (nb2 - hz);
-        c2 = idhx * (hy - nb1) + d1 * (oth0[ih - W] - hx);
+        c1 = d2 * (hx - oth0[ih - 1]) + dx * (nb2 - hz);
+        c2 = dx * (hy - nb1) + d1 * (oth0[ih - W] - hx);
         nb1 = hy;
         nb2 = hz;
       } else {
-        // curl E (src/grid.h:264-283): neighbours at j+1, k+1; nb = E of
-        // plane i+1.
-        const T idex = ld(g.ide[0] + i);
+        // curl E (src/grid.h:264-283): neighbours at j+1, k+1, and the i+1
+        // plane's Ey, Ez from the previous (higher) plane.
         const T ex = oth0[ih], ey = oth1[ih], ez = oth2[ih];
         c0 = d2 * (oth1[ih + 1] - ey) + d1 * (ez - oth2[ih + W]);
-        c1 = idex * (nb2 - ez) + d2 * (ex - oth0[ih + 1]);
-        c2 = d1 * (oth0[ih + W] - ex) + idex * (ey - nb1);
+        c1 = dx * (nb2 - ez) + d2 * (ex - oth0[ih + 1]);
+        c2 = d1 * (oth0[ih + W] - ex) + dx * (ey - nb1);
         nb1 = ey;
         nb2 = ez;
       }
-      if (!PML) {
-        if (ESWEEP) {
-          if (s0) F0[x] = cf[0] * v0 + cf[3] * c0;
-          if (s1) F1[x] = cf[1] * v1 + cf[4] * c1;
-          if (s2) F2[x] = cf[2] * v2 + cf[5] * c2;
-        } else {
-          if (s0) F0[x] = v0 + cf[0] * c0;
-          if (s1) F1[x] = v1 + cf[1] * c1;
-          if (s2) F2[x] = v2 + cf[2] * c2;
-        }
-      } else {
+      T ax0 = 0, ax1 = 0, ax2 = 0, ax3 = 0, ax4 = 0, ax5 = 0;
+      if (PML && (sel & 56u)) {
+        // Narrow boxes cover exactly the UPML points' columns.
         const T *ax = (const T *)(sc + L::OFF_AUX);
-        const int ab = (int)(round128(L::OWN_B) / sizeof(T));  // elements between aux boxes
-        const T ad0 = ld(pf.ad[0] + i), bd0 = ld(pf.bd[0] + i), ah0 = ld(pf.ah[0] + i);
-        const T ad1 = ld(pf.ad[1] + jc), bd1 = ld(pf.bd[1] + jc), ah1 = ld(pf.ah[1] + jc);
-        const T ad2 = ld(pf.ad[2] + kc), bd2 = ld(pf.bd[2] + kc), ah2 = ld(pf.ah[2] + kc);
+        constexpr int ab = (int)(round128(L::OWN_B) / sizeof(T));  // elements between aux boxes
+        ax0 = ax[ia];
+        ax1 = ax[ab + ia];
+        ax2 = ax[2 * ab + ia];
+        if (ESWEEP) {
+          ax3 = ax[3 * ab + ia];
+          ax4 = ax[4 * ab + ia];
+          ax5 = ax[5 * ab + ia];
+        }
+      }
+      // Every read of this stage is done: hand it back to the producer.
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[slot]);
+      gs++;
+
+      const int64_t x = x0 + (int64_t)i * g.s0;
+      if (ESWEEP) {
+        if (sel & 1u) F0[x] = cf[0] * v0 + cf[3] * c0;
+        if (sel & 2u) F1[x] = cf[1] * v1 + cf[4] * c1;
+        if (sel & 4u) F2[x] = cf[2] * v2 + cf[5] * c2;
+      } else {
+        if (sel & 1u) F0[x] = v0 + cf[0] * c0;
+        if (sel & 2u) F1[x] = v1 + cf[1] * c1;
+        if (sel & 4u) F2[x] = v2 + cf[2] * c2;
+      }
+      if (PML) {
+        const T xa = __shfl_sync(0xffffffffu, pa_l, p), xb = __shfl_sync(0xffffffffu, pb_l, p);
+        const T xc = __shfl_sync(0xffffffffu, pc_l, p), xd = __shfl_sync(0xffffffffu, pd_l, p);
         if (ESWEEP) {
           // src/pml.c:859-1023: PP = alpha PP + beta curl; P from PP's
-          // change; E from P's change.
-          const T ibh0 = ld(pf.ibh[0] + i), ibh1 = ld(pf.ibh[1] + jc), ibh2 = ld(pf.ibh[2] + kc);
-          if (s0) {
-            const T oPP = ax[io], oP = ax[3 * ab + io];
-            const T nPP = cf[0] * oPP + cf[3] * c0;
+          // change; E from P's change.  (a, b, c, d) = (ad, bd, ah, ibh).
+          if (sel & 8u) {
+            const T nPP = cf[0] * ax0 + cf[3] * c0;
             pf.aux[0][x] = nPP;
-            const T nP = ad1 * oP + bd1 * (nPP - oPP);
+            const T nP = q1a * ax3 + q1b * (nPP - ax0);
             pf.aux[3][x] = nP;
-            F0[x] = ad2 * v0 + bd2 * ibh0 * (nP - ah0 * oP);
+            F0[x] = q2a * v0 + q2b * xd * (nP - xc * ax3);
           }
-          if (s1) {
-            const T oPP = ax[ab + io], oP = ax[4 * ab + io];
-            const T nPP = cf[1] * oPP + cf[4] * c1;
+          if (sel & 16u) {
+            const T nPP = cf[1] * ax1 + cf[4] * c1;
             pf.aux[1][x] = nPP;
-            const T nP = ad2 * oP + bd2 * (nPP - oPP);
+            const T nP = q2a * ax4 + q2b * (nPP - ax1);
             pf.aux[4][x] = nP;
-            F1[x] = ad0 * v1 + bd0 * ibh1 * (nP - ah1 * oP);
+            F1[x] = xa * v1 + xb * q1d * (nP - q1c * ax4);
           }
-          if (s2) {
-            const T oPP = ax[2 * ab + io], oP = ax[5 * ab + io];
-            const T nPP = cf[2] * oPP + cf[5] * c2;
+          if (sel & 32u) {
+            const T nPP = cf[2] * ax2 + cf[5] * c2;
             pf.aux[2][x] = nPP;
-            const T nP = ad0 * oP + bd0 * (nPP - oPP);
+            const T nP = xa * ax5 + xb * (nPP - ax2);
             pf.aux[5][x] = nP;
-            F2[x] = ad1 * v2 + bd1 * ibh2 * (nP - ah2 * oP);
+            F2[x] = q1a * v2 + q1b * q2d * (nP - q2c * ax5);
           }
         } else {
-          // src/pml.c:1026-1176: B = ah B + gamma bh curl; H from B's change.
-          const T bh0 = ld(pf.bh[0] + i), bh1 = ld(pf.bh[1] + jc), bh2 = ld(pf.bh[2] + kc);
-          const T ibd0 = ld(pf.ibd[0] + i), ibd1 = ld(pf.ibd[1] + jc), ibd2 = ld(pf.ibd[2] + kc);
-          if (s0) {
-            const T oB = ax[io];
-            const T nB = ah1 * oB + cf[0] * bh1 * c0;
+          // src/pml.c:1026-1176: B = ah B + gamma bh curl; H from B's
+          // change.  (a, b, c, d) = (ah, bh, ad, ibd).
+          if (sel & 8u) {
+            const T nB = q1a * ax0 + cf[0] * q1b * c0;
             pf.aux[0][x] = nB;
-            F0[x] = ah2 * v0 + bh2 * ibd0 * (nB - ad0 * oB);
+            F0[x] = q2a * v0 + q2b * xd * (nB - xc * ax0);
           }
-          if (s1) {
-            const T oB = ax[ab + io];
-            const T nB = ah2 * oB + cf[1] * bh2 * c1;
+          if (sel & 16u) {
+            const T nB = q2a * ax1 + cf[1] * q2b * c1;
             pf.aux[1][x] = nB;
-            F1[x] = ah0 * v1 + bh0 * ibd1 * (nB - ad1 * oB);
+            F1[x] = xa * v1 + xb * q1d * (nB - q1c * ax1);
           }
-          if (s2) {
-            const T oB = ax[2 * ab + io];
-            const T nB = ah0 * oB + cf[2] * bh0 * c2;
+          if (sel & 32u) {
+            const T nB = xa * ax2 + cf[2] * xb * c2;
             pf.aux[2][x] = nB;
-            F2[x] = ah1 * v2 + bh1 * ibd2 * (nB - ad2 * oB);
+            F2[x] = q1a * v2 + q1b * q2d * (nB - q2c * ax2);
           }
         }
       }
     }
-    cg += n + 1;
-  }
-
-  if (failed && tid == 0) {
-    // Record the failure, then let the loads still in flight land before
-    // the block's shared memory is released.
-    atomicCAS(err, 0, 1);
-    for (int64_t q = waited; q < issued; q++) (void)mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
   }
 }
 

@@ -218,6 +218,12 @@ class GpuRun:
         N.check_gpu(N.lib().vgpu_time_kernel(self._e, kernel, warmup, iters, C.byref(ms), C.byref(pts)))
         return ms.value, pts.value
 
+    def sweep_points(self, kernel: int):
+        """(bulk, UPML) field points one sweep kernel updates per launch."""
+        b, q = C.c_uint64(), C.c_uint64()
+        N.check_gpu(N.lib().vgpu_sweep_points(self._e, kernel, C.byref(b), C.byref(q)))
+        return b.value, q.value
+
     def check_finite(self):
         N.check_gpu(N.lib().vgpu_check_finite(self._e))
 
