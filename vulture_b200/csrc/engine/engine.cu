@@ -45,7 +45,9 @@ extern "C" const char *vgpu_last_error(void) { return g_err; }
 static const int kChunk = 64;      // steps per captured graph and per DFT block
 static const int kTB = kChunk;     // DFT staging rows
 
-__global__ void k_advance(uint64_t *step) { *step += 1; }
+// The device step counter moves once per block of steps; kernels inside
+// the block add their step's offset (step_rel).
+__global__ void k_advance(uint64_t *step, int nsteps) { *step += nsteps; }
 
 struct DevAlloc {
   std::vector<void *> ptrs;
@@ -95,6 +97,7 @@ struct PwLaunch {
   PwView<T> pv;
   TfsfView te, th;
   int64_t total_e = 0, total_h = 0;
+  TfsfList<T> le{}, lh{};   // point lists of the E and H corrections
 };
 
 template <typename T>
@@ -574,8 +577,83 @@ struct Engine : EngineBase {
           }
         }
       }
+      if (int rc = build_tfsf_list(L, true)) return rc;
+      if (int rc = build_tfsf_list(L, false)) return rc;
       pws.push_back(L);
     }
+    return 0;
+  }
+
+  // The point list of one plane wave's E or H corrections (TfsfList):
+  // entries in the reference's face order, grouped by point, with the
+  // step-independent part of each incident field precomputed on the device.
+  int build_tfsf_list(PwLaunch<T> &L, bool efield)
+  {
+    const TfsfView &tv = efield ? L.te : L.th;
+    TfsfList<T> &tl = efield ? L.le : L.lh;
+    struct Ent {
+      int64_t x;
+      int c, q, axis, gi;
+      int s[3];
+      int64_t hq;
+    };
+    std::vector<Ent> ents;
+    for (int q = 0; q < tv.n; q++) {
+      const TfsfItem &it = tv.it[q];
+      for (int i = it.b.i0; i <= it.b.i1; i++)
+        for (int j = it.b.j0; j <= it.b.j1; j++)
+          for (int k = it.b.k0; k <= it.b.k1; k++) {
+            Ent e;
+            e.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
+            e.c = it.c;
+            e.q = q;
+            e.axis = it.axis;
+            e.gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
+            e.s[0] = i; e.s[1] = j; e.s[2] = k;
+            e.s[it.axis] += it.shift;
+            e.hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
+            ents.push_back(e);
+          }
+    }
+    std::stable_sort(ents.begin(), ents.end(), [](const Ent &a, const Ent &b) {
+      return a.c != b.c ? a.c < b.c : a.x < b.x;
+    });
+    const size_t ne = ents.size();
+    std::vector<int64_t> x(ne);
+    std::vector<uint8_t> q(ne);
+    std::vector<int> pos(3 * ne), gstart;
+    std::vector<T> idv(ne), ca(ne), cb(ne);
+    for (size_t e = 0; e < ne; e++) {
+      const Ent &en = ents[e];
+      if (e == 0 || en.x != ents[e - 1].x || en.c != ents[e - 1].c) gstart.push_back((int)e);
+      x[e] = en.x;
+      q[e] = (uint8_t)en.q;
+      for (int a = 0; a < 3; a++) pos[3 * e + a] = en.s[a];
+      idv[e] = (T)(efield ? p.idh[en.axis][en.gi] : p.ide[en.axis][en.gi]);
+      ca[e] = efield ? (T)p.coef[en.c][en.hq] : (T)0;
+      cb[e] = efield ? (T)p.coef[3 + en.c][en.hq] : (T)p.coef[6 + en.c - HX][en.hq];
+    }
+    gstart.push_back((int)ne);
+    tl.nentries = (int64_t)ne;
+    tl.ngroups = (int)gstart.size() - 1;
+    if (!ne) return 0;
+    int64_t *dx_;
+    uint8_t *dq;
+    int *dpos, *dg;
+    T *di, *da, *db;
+    if (upload(&dx_, x.data(), ne) || upload(&dq, q.data(), ne) || upload(&dpos, pos.data(), 3 * ne) ||
+        upload(&dg, gstart.data(), gstart.size()) || upload(&di, idv.data(), ne) || upload(&da, ca.data(), ne) ||
+        upload(&db, cb.data(), ne))
+      return VGPU_ENOMEM;
+    tl.x = dx_; tl.q = dq; tl.pos = dpos; tl.gstart = dg; tl.idv = di; tl.ca = da; tl.cb = db;
+    if (L.pv.use_aux) {
+      if (mem.alloc(&tl.cell, ne) || mem.alloc(&tl.frac, ne)) return VGPU_ENOMEM;
+    } else {
+      if (mem.alloc(&tl.dv, ne)) return VGPU_ENOMEM;
+    }
+    k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, s>>>(L.pv, tv, tl);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
     return 0;
   }
 
@@ -1039,19 +1117,20 @@ struct Engine : EngineBase {
 
   static unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
-  // One time step, in the order of src/simulation.c:156-222.
-  int enqueue_step()
+  // One time step, in the order of src/simulation.c:156-222, `rel` steps
+  // past the device step counter.
+  int enqueue_step(int rel)
   {
     uint64_t launches = 0;
     const dim3 blk(32, 8);
     if (p.num_td || p.num_fd) {
       int nt = (p.num_td + p.num_fd) * 6;
       k_observe<T><<<blocks_for(nt, 128), 128, 0, s>>>(g, d_td_pts, p.num_td, d_fd_pts, p.num_fd, d_td, d_stage, d_step,
-                                                        0, p.out_start, p.out_stop, kTB);
+                                                        rel, p.out_start, p.out_stop, kTB);
       launches++;
     }
     if (p.num_bin > 0) {
-      k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step,
+      k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step, rel,
                                                                       p.out_start, p.out_stop, kChunk);
       launches++;
     }
@@ -1071,13 +1150,13 @@ struct Engine : EngineBase {
     }
     for (auto &l : srcs)
       if (l.c <= EZ) {
-        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, 0);
+        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, rel);
         launches++;
       }
     for (auto &w : pws) {
-      if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, 0); launches++; }
+      if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, rel); launches++; }
       if (w.total_e) {
-        k_tfsf<T><<<blocks_for(w.total_e, 128), 128, 0, s>>>(g, w.pv, w.te, w.total_e, p.dt, d_step, 0, 1);
+        k_tfsf_list<T><<<blocks_for(w.le.ngroups, 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
         launches++;
       }
     }
@@ -1094,13 +1173,13 @@ struct Engine : EngineBase {
     }
     for (auto &l : srcs)
       if (l.c > EZ) {
-        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, 0);
+        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, rel);
         launches++;
       }
     for (auto &w : pws) {
       if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
       if (w.total_h) {
-        k_tfsf<T><<<blocks_for(w.total_h, 128), 128, 0, s>>>(g, w.pv, w.th, w.total_h, p.dt, d_step, 0, 0);
+        k_tfsf_list<T><<<blocks_for(w.lh.ngroups, 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
         launches++;
       }
     }
@@ -1108,9 +1187,16 @@ struct Engine : EngineBase {
       k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 12), 128, 0, s>>>(g, gv, 0, 0);
       launches++;
     }
-    k_advance<<<1, 1, 0, s>>>(d_step);
-    launches++;
     launches_per_step = launches;
+    return 0;
+  }
+
+  // `m` steps and the counter's advance past them.
+  int enqueue_steps(int m)
+  {
+    for (int q = 0; q < m; q++)
+      if (int rc = enqueue_step(q)) return rc;
+    k_advance<<<1, 1, 0, s>>>(d_step, m);
     return 0;
   }
 
@@ -1118,7 +1204,7 @@ struct Engine : EngineBase {
   {
     cudaGraph_t gr;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int q = 0; q < kChunk; q++) enqueue_step();
+    enqueue_steps(kChunk);
     CK(cudaStreamEndCapture(s, &gr));
     cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
     cudaGraphDestroy(gr);
@@ -1165,9 +1251,9 @@ struct Engine : EngineBase {
       if (m == (uint64_t)kChunk) {
         CK(cudaGraphLaunch(graph, s));
       } else {
-        for (uint64_t q = 0; q < m; q++) enqueue_step();
+        if (int rc = enqueue_steps((int)m)) return rc;
       }
-      launches += m * launches_per_step;
+      launches += m * launches_per_step + 1;
       step += m;
       done += m;
       // Output rows produced in this chunk.

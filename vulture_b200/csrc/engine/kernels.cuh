@@ -311,11 +311,12 @@ __global__ void k_ghost(Grid<T> g, GhostView gv, int efield, int nb_all)
 // block (n / chunk) % 2, as float.
 template <typename T>
 __global__ void k_bin_observe(Grid<T> g, const int *__restrict__ pts, int64_t npts, float *__restrict__ ring,
-                              const uint64_t *step_base, uint64_t out_start, uint64_t out_stop, int chunk)
+                              const uint64_t *step_base, int step_rel, uint64_t out_start, uint64_t out_stop,
+                              int chunk)
 {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * 6) return;
-  const uint64_t n = *step_base;
+  const uint64_t n = *step_base + step_rel;
   if (n < out_start || n > out_stop) return;
   const int64_t q = t / 6;
   const int c = (int)(t - q * 6);
@@ -415,16 +416,21 @@ __device__ inline double dev_spline(const DevWaveform &w, double t)
          ((a * a * a - a) * tab[3 * klo + 2] + (b * b * b - b) * tab[3 * khi + 2]) * (h * h) / 6.0;
 }
 
+// The reference squares with pow(v, 2.0); v * v is the correctly rounded
+// square, which a correctly rounded pow also returns, at a fraction of the
+// cost.
+__device__ __forceinline__ double sq(double v) { return v * v; }
+
 __device__ inline double dev_waveform(const DevWaveform &w, double t, double delay)
 {
   const double pi = 3.14159265358979311600;  // 4*atan(1) in double
   double x = t - delay - w.delay, W = w.width, f = w.frequency, env;
   switch (w.type) {
     case VGPU_WF_GAUSSIAN_PULSE:
-    case VGPU_WF_NARROW_GAUSSIAN_PULSE: return w.size * exp(-0.5 * (pow(x / W, 2.0)));
-    case VGPU_WF_DIFF_GAUSSIAN_PULSE: return w.size * (-x / W * exp(-0.5 * (pow(x / W, 2.0))));
-    case VGPU_WF_RICKER_WAVELET: return w.size * ((1.0 - pow(x / W, 2.0)) * exp(-0.5 * (pow(x / W, 2.0))));
-    case VGPU_WF_MOD_GAUSSIAN_PULSE: return w.size * (exp(-0.5 * (pow(x / W, 2.0))) * sin(2.0 * pi * f * x));
+    case VGPU_WF_NARROW_GAUSSIAN_PULSE: return w.size * exp(-0.5 * sq(x / W));
+    case VGPU_WF_DIFF_GAUSSIAN_PULSE: return w.size * (-x / W * exp(-0.5 * sq(x / W)));
+    case VGPU_WF_RICKER_WAVELET: return w.size * ((1.0 - sq(x / W)) * exp(-0.5 * sq(x / W)));
+    case VGPU_WF_MOD_GAUSSIAN_PULSE: return w.size * (exp(-0.5 * sq(x / W)) * sin(2.0 * pi * f * x));
     case VGPU_WF_COMPACT_PULSE:
     case VGPU_WF_MOD_COMPACT_PULSE:
       if (x <= 0.0) env = 0.0;
@@ -478,39 +484,6 @@ struct TfsfView {
   TfsfItem it[12];
 };
 
-template <typename T>
-__device__ inline T incident_field(const PwView<T> &pw, int c, int i, int j, int k, double time)
-{
-  if (!pw.use_aux) {
-    int g[3] = { i, j, k };
-    double r[3];
-    for (int a = 0; a < 3; a++) {
-      bool half = c <= EZ ? (c == a) : (c - HX != a);
-      r[a] = half ? pw.pos_half[a][g[a]] : pw.pos_node[a][g[a]];
-    }
-    double d = pw.kinc[0] * (r[0] - pw.r0[0]) + pw.kinc[1] * (r[1] - pw.r0[1]) + pw.kinc[2] * (r[2] - pw.r0[2]);
-    return (T)(pw.finc[c] * dev_waveform(pw.wf, time - d / pw.phase_velocity, pw.delay));
-  }
-  T rc[3] = { (T)i, (T)j, (T)k };
-  if (c <= EZ) rc[c] = rc[c] + (T)0.5;
-  else
-    for (int a = 0; a < 3; a++)
-      if (a != c - HX) rc[a] = rc[a] + (T)0.5;
-  T d = (T)pw.kinc[0] * (rc[0] - (T)pw.ijk0[0]) + (T)pw.kinc[1] * (rc[1] - (T)pw.ijk0[1]) +
-        (T)pw.kinc[2] * (rc[2] - (T)pw.ijk0[2]);
-  T value;
-  if (c <= EZ) {
-    int id = (int)floor((double)d);
-    T dp = d - (T)id;
-    value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
-  } else {
-    int id = (int)floor((double)d + 0.5);
-    T dp = (T)((double)d + 0.5 - id);
-    value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
-  }
-  return (T)pw.finc[c] * value;
-}
-
 // Auxiliary 1-D grid, one block (src/planewave.c:1318-1374).
 template <typename T>
 __global__ void k_aux_e(PwView<T> pw, const uint64_t *step_base, int step_rel)
@@ -539,43 +512,100 @@ __global__ void k_aux_h(PwView<T> pw)
   }
 }
 
-// Face corrections.  A point on several faces (edges of the Huygens box) is
-// corrected by the thread of its first face, which applies all of its faces
-// in the reference's order (YLO, YHI, ZLO, ZHI, XLO, XHI).
+// Face corrections from a precomputed point list.  Each entry is one
+// (face, point) correction of the reference's loops; the entries of one
+// point are contiguous, in the reference's face order, and form a group that
+// one thread applies in sequence.  What does not change between steps is
+// computed once by k_tfsf_prepare -- the analytic field's phase term
+// d / v, or the auxiliary-grid cell and fraction -- and the line length and
+// update coefficients are copies of the grid's values.
 template <typename T>
-__global__ void k_tfsf(Grid<T> g, PwView<T> pw, TfsfView tv, int64_t total, double dt, const uint64_t *step_base,
-                       int step_rel, int efield)
+struct TfsfList {
+  const int64_t *x;        // field index of the corrected point
+  const uint8_t *q;        // item (face, component) of the entry
+  const int *pos;          // incident-field position, 3 ints per entry
+  double *dv;              // analytic field: d / phase velocity
+  int *cell;               // auxiliary grid: cell
+  T *frac;                 // auxiliary grid: fraction
+  const T *idv, *ca, *cb;  // line length; alpha and beta (E) or gamma (H)
+  const int *gstart;       // group starts, ngroups + 1 entries
+  int64_t nentries;
+  int ngroups;
+};
+
+template <typename T>
+__global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
 {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  int q = 0;
-  while (q + 1 < tv.n && t >= tv.it[q + 1].first) q++;
-  const TfsfItem &m = tv.it[q];
-  int64_t u = t - m.first, nj = m.b.nj(), nk = m.b.nk();
-  int i = m.b.i0 + (int)(u / (nj * nk)), j = m.b.j0 + (int)((u / nk) % nj), k = m.b.k0 + (int)(u % nk);
-  for (int e = 0; e < q; e++)
-    if (tv.it[e].c == m.c && tv.it[e].b.contains(i, j, k)) return;
-  uint64_t n = *step_base + step_rel;
-  double time = efield ? n * dt : (n + 0.5) * dt;
-  const int64_t x = g.at(i, j, k);
-  T *F = g.F[m.c];
-  for (int e = q; e < tv.n; e++) {
-    const TfsfItem &it = tv.it[e];
-    if (it.c != m.c || !it.b.contains(i, j, k)) continue;
-    int s[3] = { i, j, k };
-    s[it.axis] += it.shift;
-    T inc = incident_field(pw, it.inc, s[0], s[1], s[2], time);
-    int gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
-    if (efield) {
-      T al = g.cf[it.c][x], be = g.cf[3 + it.c][x], idv = g.idh[it.axis][gi];
-      if (it.sign > 0) F[x] = al * F[x] + be * (idv * inc);
-      else F[x] = al * F[x] - be * (idv * inc);
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= tl.nentries) return;
+  const int c = tv.it[tl.q[e]].inc;
+  const int i = tl.pos[3 * e], j = tl.pos[3 * e + 1], k = tl.pos[3 * e + 2];
+  if (!pw.use_aux) {
+    // Phase term of the analytic incident field (src/planewave.c:450-554):
+    // d = kinc . (r - r0), r at the component's node or mid-edge position.
+    int gg[3] = { i, j, k };
+    double r[3];
+    for (int a = 0; a < 3; a++) {
+      bool half = c <= EZ ? (c == a) : (c - HX != a);
+      r[a] = half ? pw.pos_half[a][gg[a]] : pw.pos_node[a][gg[a]];
+    }
+    double d = pw.kinc[0] * (r[0] - pw.r0[0]) + pw.kinc[1] * (r[1] - pw.r0[1]) + pw.kinc[2] * (r[2] - pw.r0[2]);
+    tl.dv[e] = d / pw.phase_velocity;
+    return;
+  }
+  T rc[3] = { (T)i, (T)j, (T)k };
+  if (c <= EZ) rc[c] = rc[c] + (T)0.5;
+  else
+    for (int a = 0; a < 3; a++)
+      if (a != c - HX) rc[a] = rc[a] + (T)0.5;
+  T d = (T)pw.kinc[0] * (rc[0] - (T)pw.ijk0[0]) + (T)pw.kinc[1] * (rc[1] - (T)pw.ijk0[1]) +
+        (T)pw.kinc[2] * (rc[2] - (T)pw.ijk0[2]);
+  if (c <= EZ) {
+    int id = (int)floor((double)d);
+    tl.cell[e] = id;
+    tl.frac[e] = d - (T)id;
+  } else {
+    int id = (int)floor((double)d + 0.5);
+    tl.cell[e] = id;
+    tl.frac[e] = (T)((double)d + 0.5 - id);
+  }
+}
+
+template <typename T>
+__global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, double dt,
+                            const uint64_t *step_base, int step_rel, int efield)
+{
+  const int grp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (grp >= tl.ngroups) return;
+  const int e0 = tl.gstart[grp], e1 = tl.gstart[grp + 1];
+  const uint64_t n = *step_base + step_rel;
+  const double time = efield ? n * dt : (n + 0.5) * dt;
+  const int64_t x = tl.x[e0];
+  T *F = g.F[tv.it[tl.q[e0]].c];
+  T v = F[x];
+  for (int e = e0; e < e1; e++) {
+    const TfsfItem &it = tv.it[tl.q[e]];
+    T inc;
+    if (!pw.use_aux) {
+      inc = (T)(pw.finc[it.inc] * dev_waveform(pw.wf, time - tl.dv[e], pw.delay));
     } else {
-      T ga = g.cf[6 + it.c - HX][x], idv = g.ide[it.axis][gi];
-      if (it.sign > 0) F[x] = F[x] + ga * (idv * inc);
-      else F[x] = F[x] - ga * (idv * inc);
+      const int id = tl.cell[e];
+      const T dp = tl.frac[e];
+      T value;
+      if (it.inc <= EZ) value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
+      else value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
+      inc = (T)pw.finc[it.inc] * value;
+    }
+    const T idv = tl.idv[e];
+    if (efield) {
+      if (it.sign > 0) v = tl.ca[e] * v + tl.cb[e] * (idv * inc);
+      else v = tl.ca[e] * v - tl.cb[e] * (idv * inc);
+    } else {
+      if (it.sign > 0) v = v + tl.cb[e] * (idv * inc);
+      else v = v - tl.cb[e] * (idv * inc);
     }
   }
+  F[x] = v;
 }
 
 // ---------------------------------------------------------------------------
