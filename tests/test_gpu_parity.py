@@ -89,6 +89,25 @@ def test_fp32_within_1e4_of_fp64(case):
         assert rel_l2(a[:, p, :], b[:, p, :]) <= 1e-4, f"observer {p}"
 
 
+def many_media_mesh(nmedia=300, seed=5):
+    """A mesh with more distinct coefficient tuples than the one-byte index
+    holds, so the sweeps read the full coefficient volumes: single-cell
+    blocks of seeded dielectrics and conductors inside a UPML box."""
+    rng = random.Random(seed)
+    out = ["VM 1.0.0", "CE many media", "DM 24 22 20", "GS",
+           "BT XLO PML 4", "BT XHI PML 4", "BT YLO PML 4", "BT YHI PML 4", "BT ZLO PML 4", "BT ZHI PML 4"]
+    for m in range(nmedia):
+        out.append(f"MT m{m} SIMPLE {1.0 + 9.0 * rng.random():.6f} {0.05 * rng.random():.6f} 1.0")
+    cells = set()
+    while len(cells) < nmedia:
+        cells.add((rng.randrange(3, 21), rng.randrange(3, 19), rng.randrange(3, 17)))
+    for m, (i, j, k) in enumerate(sorted(cells)):
+        out.append(f"MB {i} {i + 1} {j} {j + 1} {k} {k + 1} m{m}")
+    out += ["WF wf1 GAUSSIAN_PULSE 1.0", "EX 12 12 11 11 10 11 src =EZ wf1 1.0",
+            "OP 8 8 8 8 8 8 op1 TDOM_ASCII", "OP 15 15 14 14 12 12 op2 TDOM_ASCII", "GE", "NT 120", "MS 0.01", "EN"]
+    return "\n".join(out) + "\n"
+
+
 def synthetic():
     rng = random.Random(11)
     return {
@@ -97,6 +116,7 @@ def synthetic():
         "config3_small": meshgen.config3(nt=150, dims=(80, 64, 56), plane=8, nfreq=20),
         "config4_mesh": meshgen.config4_mesh(rng, 0, nmin=32, nmax=64, ntmin=200, ntmax=300),
         "config5_req": meshgen.config5_request(rng, 0, nmin=48, nmax=64, ntmin=200, ntmax=300),
+        "many_media": many_media_mesh(),
     }
 
 

@@ -243,11 +243,22 @@ struct Engine : EngineBase {
     if (mem.alloc(&fields, (size_t)vol * 6)) return VGPU_ENOMEM;
     CK(cudaMemset(fields, 0, sizeof(T) * vol * 6));
     for (int c = 0; c < 6; c++) g.F[c] = fields + (int64_t)c * vol;
-    T *coef = nullptr;
-    if (mem.alloc(&coef, (size_t)vol * 9)) return VGPU_ENOMEM;
-    for (int q = 0; q < 9; q++) {
-      if (int rc = upload_volume(coef + (int64_t)q * vol, p.coef[q])) return rc;
-      g.cf[q] = coef + (int64_t)q * vol;
+    // Coefficients: a one-byte index and a table where the mesh allows it
+    // (at most 256 distinct tuples), else the full volumes.
+    if (int rc = setup_coef_index()) return rc;
+    g.cidx[0] = cie.idx;
+    g.ctab[0] = (const T *)cie.table;
+    g.cidx[1] = cih.idx;
+    g.ctab[1] = (const T *)cih.table;
+    for (int grp = 0; grp < 2; grp++) {
+      if ((grp == 0 ? cie : cih).idx) continue;
+      const int q0 = grp == 0 ? 0 : 6, nq = grp == 0 ? 6 : 3;
+      T *coef = nullptr;
+      if (mem.alloc(&coef, (size_t)vol * nq)) return VGPU_ENOMEM;
+      for (int q = 0; q < nq; q++) {
+        if (int rc = upload_volume(coef + (int64_t)q * vol, p.coef[q0 + q])) return rc;
+        g.cf[q0 + q] = coef + (int64_t)q * vol;
+      }
     }
     for (int a = 0; a < 3; a++) {
       T *d;
@@ -275,7 +286,6 @@ struct Engine : EngineBase {
     if (int rc = setup_planewaves()) return rc;
     setup_ghost();
     if (int rc = setup_observers()) return rc;
-    if (int rc = setup_coef_index()) return rc;
     if (int rc = setup_sweeps()) return rc;
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
@@ -618,39 +628,49 @@ struct Engine : EngineBase {
     std::stable_sort(ents.begin(), ents.end(), [](const Ent &a, const Ent &b) {
       return a.c != b.c ? a.c < b.c : a.x < b.x;
     });
+    // Points of one entry first, then the multi-entry points' runs.
     const size_t ne = ents.size();
-    std::vector<int64_t> x(ne);
-    std::vector<uint8_t> q(ne);
-    std::vector<int> pos(3 * ne), gstart;
-    std::vector<T> idv(ne), ca(ne), cb(ne);
-    for (size_t e = 0; e < ne; e++) {
-      const Ent &en = ents[e];
-      if (e == 0 || en.x != ents[e - 1].x || en.c != ents[e - 1].c) gstart.push_back((int)e);
-      x[e] = en.x;
-      q[e] = (uint8_t)en.q;
-      for (int a = 0; a < 3; a++) pos[3 * e + a] = en.s[a];
-      idv[e] = (T)(efield ? p.idh[en.axis][en.gi] : p.ide[en.axis][en.gi]);
-      ca[e] = efield ? (T)p.coef[en.c][en.hq] : (T)0;
-      cb[e] = efield ? (T)p.coef[3 + en.c][en.hq] : (T)p.coef[6 + en.c - HX][en.hq];
+    std::vector<size_t> order;
+    std::vector<int> mstart;
+    order.reserve(ne);
+    std::vector<std::pair<size_t, size_t>> runs;
+    for (size_t e = 0; e < ne;) {
+      size_t f = e + 1;
+      while (f < ne && ents[f].x == ents[e].x && ents[f].c == ents[e].c) f++;
+      if (f - e == 1) order.push_back(e);
+      else runs.push_back({ e, f });
+      e = f;
     }
-    gstart.push_back((int)ne);
+    const int nsingle = (int)order.size();
+    for (auto &r : runs) {
+      mstart.push_back((int)order.size());
+      for (size_t e = r.first; e < r.second; e++) order.push_back(e);
+    }
+    mstart.push_back((int)order.size());
+    std::vector<TfsfEntry<T>> ent(ne);
+    std::vector<int> pos(3 * ne);
+    for (size_t o = 0; o < ne; o++) {
+      const Ent &en = ents[order[o]];
+      TfsfEntry<T> &d = ent[o];
+      memset(&d, 0, sizeof d);
+      d.x = en.x;
+      d.q = en.q;
+      d.idv = (T)(efield ? p.idh[en.axis][en.gi] : p.ide[en.axis][en.gi]);
+      d.ca = efield ? (T)p.coef[en.c][en.hq] : (T)0;
+      d.cb = efield ? (T)p.coef[3 + en.c][en.hq] : (T)p.coef[6 + en.c - HX][en.hq];
+      for (int a = 0; a < 3; a++) pos[3 * o + a] = en.s[a];
+    }
     tl.nentries = (int64_t)ne;
-    tl.ngroups = (int)gstart.size() - 1;
+    tl.nsingle = nsingle;
+    tl.nmulti = (int)runs.size();
     if (!ne) return 0;
-    int64_t *dx_;
-    uint8_t *dq;
-    int *dpos, *dg;
-    T *di, *da, *db;
-    if (upload(&dx_, x.data(), ne) || upload(&dq, q.data(), ne) || upload(&dpos, pos.data(), 3 * ne) ||
-        upload(&dg, gstart.data(), gstart.size()) || upload(&di, idv.data(), ne) || upload(&da, ca.data(), ne) ||
-        upload(&db, cb.data(), ne))
+    TfsfEntry<T> *de;
+    int *dpos, *dm;
+    if (upload(&de, ent.data(), ne) || upload(&dpos, pos.data(), 3 * ne) || upload(&dm, mstart.data(), mstart.size()))
       return VGPU_ENOMEM;
-    tl.x = dx_; tl.q = dq; tl.pos = dpos; tl.gstart = dg; tl.idv = di; tl.ca = da; tl.cb = db;
-    if (L.pv.use_aux) {
-      if (mem.alloc(&tl.cell, ne) || mem.alloc(&tl.frac, ne)) return VGPU_ENOMEM;
-    } else {
-      if (mem.alloc(&tl.dv, ne)) return VGPU_ENOMEM;
-    }
+    tl.ent = de;
+    tl.pos = dpos;
+    tl.mstart = dm;
     k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, s>>>(L.pv, tv, tl);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -748,11 +768,13 @@ struct Engine : EngineBase {
       if (int rc = make_map(&m.oth[c], g.F[(esweep ? HX : EX) + c], dt, e, wc, jh + 1)) return rc;
     }
     const int ncoef = esweep ? 6 : 3;
-    for (int c = 0; c < ncoef; c++)
-      if (int rc = make_map(&m.coef[c], g.cf[(esweep ? 0 : 6) + c], dt, e, w, jh)) return rc;
     const CoefIndex &ci = esweep ? cie : cih;
-    if (ci.idx)
+    if (ci.idx) {
       if (int rc = make_map(&m.idx, ci.idx, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, 32, jh)) return rc;
+    } else {
+      for (int c = 0; c < ncoef; c++)
+        if (int rc = make_map(&m.coef[c], g.cf[(esweep ? 0 : 6) + c], dt, e, w, jh)) return rc;
+    }
     if (has_pml) {
       const PmlFull<T> &pf = esweep ? pfe : pfh;
       for (int c = 0; c < (esweep ? 6 : 3); c++) {
@@ -1017,7 +1039,6 @@ struct Engine : EngineBase {
 
   int setup_coef_index()
   {
-    if (getenv("VGPU_FULL_COEFFICIENTS")) return 0;
     if (int rc = build_index(0, 6, cie)) return rc;
     return build_index(6, 3, cih);
   }
@@ -1156,7 +1177,7 @@ struct Engine : EngineBase {
     for (auto &w : pws) {
       if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, rel); launches++; }
       if (w.total_e) {
-        k_tfsf_list<T><<<blocks_for(w.le.ngroups, 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
+        k_tfsf_list<T><<<blocks_for(w.le.nsingle + w.le.nmulti, 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
         launches++;
       }
     }
@@ -1179,7 +1200,7 @@ struct Engine : EngineBase {
     for (auto &w : pws) {
       if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
       if (w.total_h) {
-        k_tfsf_list<T><<<blocks_for(w.lh.ngroups, 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
+        k_tfsf_list<T><<<blocks_for(w.lh.nsingle + w.lh.nmulti, 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
         launches++;
       }
     }

@@ -34,16 +34,27 @@ struct Box {
 static inline Box box_from(const int32_t l[6]) { return Box{ l[0], l[1], l[2], l[3], l[4], l[5] }; }
 
 // Device view of the grid: fields, coefficients and line arrays.  Volumes are
-// [n0][n1][n2p] with the k rows padded to a multiple of 32 elements.
+// [n0][n1][n2p] with the k rows padded to a multiple of 32 elements.  The E
+// (alpha, beta) and H (gamma) coefficients come either from full volumes
+// (cf) or, for meshes with at most 256 distinct tuples, from a one-byte
+// index per point and a table (cidx, ctab); coef() reads whichever is set.
 template <typename T>
 struct Grid {
   T *F[6];
   const T *cf[9];
+  const uint8_t *cidx[2];   // E, H coefficient index (null: volumes)
+  const T *ctab[2];         // tables: 6 values per E tuple, 3 per H tuple
   const T *ide[3];
   const T *idh[3];
   int n0, n1, n2;
   int64_t s0, s1;  // strides of i and j
   __device__ __forceinline__ int64_t at(int i, int j, int k) const { return (int64_t)i * s0 + (int64_t)j * s1 + k; }
+  // Coefficient q (0..5 alpha/beta E x,y,z; 6..8 gamma H x,y,z) at point x.
+  __device__ __forceinline__ T coef(int q, int64_t x) const
+  {
+    if (q < 6) return cidx[0] ? ctab[0][6 * (int)cidx[0][x] + q] : cf[q][x];
+    return cidx[1] ? ctab[1][3 * (int)cidx[1][x] + (q - 6)] : cf[q][x];
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -97,9 +108,9 @@ __device__ __forceinline__ T bulk_e_value(const Grid<T> &g, int c, int i, int j,
 {
   const int64_t x = g.at(i, j, k);
   const T *Hx = g.F[HX], *Hy = g.F[HY], *Hz = g.F[HZ];
-  if (c == EX) return g.cf[0][x] * g.F[EX][x] + g.cf[3][x] * (g.idh[1][j] * (Hz[x] - Hz[x - g.s1]) + g.idh[2][k] * (Hy[x - 1] - Hy[x]));
-  if (c == EY) return g.cf[1][x] * g.F[EY][x] + g.cf[4][x] * (g.idh[2][k] * (Hx[x] - Hx[x - 1]) + g.idh[0][i] * (Hz[x - g.s0] - Hz[x]));
-  return g.cf[2][x] * g.F[EZ][x] + g.cf[5][x] * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
+  if (c == EX) return g.coef(0, x) * g.F[EX][x] + g.coef(3, x) * (g.idh[1][j] * (Hz[x] - Hz[x - g.s1]) + g.idh[2][k] * (Hy[x - 1] - Hy[x]));
+  if (c == EY) return g.coef(1, x) * g.F[EY][x] + g.coef(4, x) * (g.idh[2][k] * (Hx[x] - Hx[x - 1]) + g.idh[0][i] * (Hz[x - g.s0] - Hz[x]));
+  return g.coef(2, x) * g.F[EZ][x] + g.coef(5, x) * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
 }
 
 template <typename T>
@@ -142,11 +153,11 @@ __global__ void k_mur_h(Grid<T> g, MurView mv, int64_t total)
   const int64_t x = g.at(i, j, k);
   const T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
   if (m.c == HX)
-    g.F[HX][x] = g.F[HX][x] + g.cf[6][x] * (g.ide[2][k] * (Ey[x + 1] - Ey[x]) + g.ide[1][j] * (Ez[x] - Ez[x + g.s1]));
+    g.F[HX][x] = g.F[HX][x] + g.coef(6, x) * (g.ide[2][k] * (Ey[x + 1] - Ey[x]) + g.ide[1][j] * (Ez[x] - Ez[x + g.s1]));
   else if (m.c == HY)
-    g.F[HY][x] = g.F[HY][x] + g.cf[7][x] * (g.ide[0][i] * (Ez[x + g.s0] - Ez[x]) + g.ide[2][k] * (Ex[x] - Ex[x + 1]));
+    g.F[HY][x] = g.F[HY][x] + g.coef(7, x) * (g.ide[0][i] * (Ez[x + g.s0] - Ez[x]) + g.ide[2][k] * (Ex[x] - Ex[x + 1]));
   else
-    g.F[HZ][x] = g.F[HZ][x] + g.cf[8][x] * (g.ide[1][j] * (Ex[x + g.s1] - Ex[x]) + g.ide[0][i] * (Ey[x] - Ey[x + g.s0]));
+    g.F[HZ][x] = g.F[HZ][x] + g.coef(8, x) * (g.ide[1][j] * (Ex[x + g.s1] - Ex[x]) + g.ide[0][i] * (Ey[x] - Ey[x + g.s0]));
 }
 
 // ---------------------------------------------------------------------------
@@ -186,7 +197,7 @@ __global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t t
     sr = sr + (ar * v.x - ai * v.y);
     si = si + (ar * v.y + ai * v.x);
   }
-  E[x] = E[x] - g.cf[3 + m.c][x] * sr;
+  E[x] = E[x] - g.coef(3 + m.c, x) * sr;
   T diff = E[x] - lastE[m.eofs + cell];
   for (int p = 0; p < m.np; p++) {
     double2 v = Jc[p];
@@ -213,7 +224,7 @@ __global__ void k_source(Grid<T> g, Box b, int c, int kind, T soft, const T *val
   T v = values[*step_base + step_rel];
   T *F = g.F[c];
   if (kind == VGPU_SRC_FIELD) F[x] = soft * F[x] + v;
-  else F[x] = soft * F[x] - g.cf[c <= EZ ? 3 + c : 6 + c - HX][x] * v;
+  else F[x] = soft * F[x] - g.coef(c <= EZ ? 3 + c : 6 + c - HX, x) * v;
 }
 
 // ---------------------------------------------------------------------------
@@ -513,24 +524,32 @@ __global__ void k_aux_h(PwView<T> pw)
 }
 
 // Face corrections from a precomputed point list.  Each entry is one
-// (face, point) correction of the reference's loops; the entries of one
-// point are contiguous, in the reference's face order, and form a group that
-// one thread applies in sequence.  What does not change between steps is
-// computed once by k_tfsf_prepare -- the analytic field's phase term
-// d / v, or the auxiliary-grid cell and fraction -- and the line length and
-// update coefficients are copies of the grid's values.
+// (face, point) correction of the reference's loops.  Points corrected by
+// one face only come first, one entry each; the entries of a point on
+// several faces (the Huygens box's edges) follow, contiguous and in the
+// reference's face order, and one thread applies them in sequence.  What
+// does not change between steps is computed once by k_tfsf_prepare: the
+// analytic field's phase term d / v, or the auxiliary-grid cell and
+// fraction.  The line length and update coefficients are copies of the
+// grid's values.
+template <typename T>
+struct alignas(16) TfsfEntry {
+  int64_t x;    // field index of the corrected point
+  double dv;    // analytic field: d / phase velocity
+  T idv;        // line length
+  T ca, cb;     // alpha and beta (E) or -, gamma (H)
+  T frac;       // auxiliary grid: fraction
+  int cell;     // auxiliary grid: cell
+  int q;        // item (face, component)
+};
+
 template <typename T>
 struct TfsfList {
-  const int64_t *x;        // field index of the corrected point
-  const uint8_t *q;        // item (face, component) of the entry
-  const int *pos;          // incident-field position, 3 ints per entry
-  double *dv;              // analytic field: d / phase velocity
-  int *cell;               // auxiliary grid: cell
-  T *frac;                 // auxiliary grid: fraction
-  const T *idv, *ca, *cb;  // line length; alpha and beta (E) or gamma (H)
-  const int *gstart;       // group starts, ngroups + 1 entries
+  TfsfEntry<T> *ent;
+  const int *pos;          // incident-field position, 3 ints per entry (set-up only)
+  const int *mstart;       // multi-entry points: entry starts, nmulti + 1 values
   int64_t nentries;
-  int ngroups;
+  int nsingle, nmulti;
 };
 
 template <typename T>
@@ -538,7 +557,8 @@ __global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
 {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= tl.nentries) return;
-  const int c = tv.it[tl.q[e]].inc;
+  TfsfEntry<T> &en = tl.ent[e];
+  const int c = tv.it[en.q].inc;
   const int i = tl.pos[3 * e], j = tl.pos[3 * e + 1], k = tl.pos[3 * e + 2];
   if (!pw.use_aux) {
     // Phase term of the analytic incident field (src/planewave.c:450-554):
@@ -550,7 +570,7 @@ __global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
       r[a] = half ? pw.pos_half[a][gg[a]] : pw.pos_node[a][gg[a]];
     }
     double d = pw.kinc[0] * (r[0] - pw.r0[0]) + pw.kinc[1] * (r[1] - pw.r0[1]) + pw.kinc[2] * (r[2] - pw.r0[2]);
-    tl.dv[e] = d / pw.phase_velocity;
+    en.dv = d / pw.phase_velocity;
     return;
   }
   T rc[3] = { (T)i, (T)j, (T)k };
@@ -562,50 +582,61 @@ __global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
         (T)pw.kinc[2] * (rc[2] - (T)pw.ijk0[2]);
   if (c <= EZ) {
     int id = (int)floor((double)d);
-    tl.cell[e] = id;
-    tl.frac[e] = d - (T)id;
+    en.cell = id;
+    en.frac = d - (T)id;
   } else {
     int id = (int)floor((double)d + 0.5);
-    tl.cell[e] = id;
-    tl.frac[e] = (T)((double)d + 0.5 - id);
+    en.cell = id;
+    en.frac = (T)((double)d + 0.5 - id);
   }
+}
+
+// One correction of `v` (src/planewave.c:576-1007, the expression of the
+// item's face and component).
+template <typename T>
+__device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv, const TfsfEntry<T> &en, T v,
+                                        double time, int efield)
+{
+  const TfsfItem &it = tv.it[en.q];
+  T inc;
+  if (!pw.use_aux) {
+    inc = (T)(pw.finc[it.inc] * dev_waveform(pw.wf, time - en.dv, pw.delay));
+  } else {
+    const int id = en.cell;
+    const T dp = en.frac;
+    T value;
+    if (it.inc <= EZ) value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
+    else value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
+    inc = (T)pw.finc[it.inc] * value;
+  }
+  if (efield) {
+    if (it.sign > 0) return en.ca * v + en.cb * (en.idv * inc);
+    return en.ca * v - en.cb * (en.idv * inc);
+  }
+  if (it.sign > 0) return v + en.cb * (en.idv * inc);
+  return v - en.cb * (en.idv * inc);
 }
 
 template <typename T>
 __global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, double dt,
                             const uint64_t *step_base, int step_rel, int efield)
 {
-  const int grp = blockIdx.x * blockDim.x + threadIdx.x;
-  if (grp >= tl.ngroups) return;
-  const int e0 = tl.gstart[grp], e1 = tl.gstart[grp + 1];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= tl.nsingle + tl.nmulti) return;
   const uint64_t n = *step_base + step_rel;
   const double time = efield ? n * dt : (n + 0.5) * dt;
-  const int64_t x = tl.x[e0];
-  T *F = g.F[tv.it[tl.q[e0]].c];
-  T v = F[x];
-  for (int e = e0; e < e1; e++) {
-    const TfsfItem &it = tv.it[tl.q[e]];
-    T inc;
-    if (!pw.use_aux) {
-      inc = (T)(pw.finc[it.inc] * dev_waveform(pw.wf, time - tl.dv[e], pw.delay));
-    } else {
-      const int id = tl.cell[e];
-      const T dp = tl.frac[e];
-      T value;
-      if (it.inc <= EZ) value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
-      else value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
-      inc = (T)pw.finc[it.inc] * value;
-    }
-    const T idv = tl.idv[e];
-    if (efield) {
-      if (it.sign > 0) v = tl.ca[e] * v + tl.cb[e] * (idv * inc);
-      else v = tl.ca[e] * v - tl.cb[e] * (idv * inc);
-    } else {
-      if (it.sign > 0) v = v + tl.cb[e] * (idv * inc);
-      else v = v - tl.cb[e] * (idv * inc);
-    }
+  if (t < tl.nsingle) {
+    const TfsfEntry<T> en = tl.ent[t];
+    T *F = g.F[tv.it[en.q].c];
+    F[en.x] = tfsf_apply(pw, tv, en, F[en.x], time, efield);
+    return;
   }
-  F[x] = v;
+  const int e0 = tl.mstart[t - tl.nsingle], e1 = tl.mstart[t - tl.nsingle + 1];
+  const TfsfEntry<T> first = tl.ent[e0];
+  T *F = g.F[tv.it[first.q].c];
+  T v = F[first.x];
+  for (int e = e0; e < e1; e++) v = tfsf_apply(pw, tv, tl.ent[e], v, time, efield);
+  F[first.x] = v;
 }
 
 // ---------------------------------------------------------------------------
