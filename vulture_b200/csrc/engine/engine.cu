@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <thread>
 
 #include "kernels.cuh"
 #include "sweep_tma.cuh"
@@ -49,23 +50,91 @@ static const int kTB = kChunk;     // DFT staging rows
 // the block add their step's offset (step_rel).
 __global__ void k_advance(uint64_t *step, int nsteps) { *step += nsteps; }
 
+// Device memory of destroyed engines is kept in a per-device cache and
+// handed to later engines that ask for a block of about the same size, so
+// that creating a problem again (tests, batches, a service) does not map new
+// pages.  The cache gives its memory back to the driver when it holds more
+// than a quarter of the device, and when an allocation would not fit.
+struct BlockCache {
+  std::mutex mu;
+  std::map<int, std::multimap<size_t, void *>> free_blocks;   // device -> size -> block
+  std::map<int, size_t> held;
+
+  // A cached block of at least b bytes (and not much more), or null; its
+  // size goes to *got.
+  void *take(int dev, size_t b, size_t *got)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto &fb = free_blocks[dev];
+    auto it = fb.lower_bound(b);
+    if (it == fb.end() || it->first > 2 * b + (1u << 20)) return nullptr;
+    void *p = it->second;
+    *got = it->first;
+    held[dev] -= it->first;
+    fb.erase(it);
+    return p;
+  }
+  void give(int dev, size_t b, void *p)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    size_t total = 0, fr = 0;
+    cudaMemGetInfo(&fr, &total);
+    free_blocks[dev].emplace(b, p);
+    held[dev] += b;
+    if (held[dev] > total / 4) release_locked(dev);
+  }
+  void release(int dev)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    release_locked(dev);
+  }
+  void release_locked(int dev)
+  {
+    for (auto &kv : free_blocks[dev]) cudaFree(kv.second);
+    free_blocks[dev].clear();
+    held[dev] = 0;
+  }
+};
+
+static BlockCache &block_cache()
+{
+  static BlockCache *c = new BlockCache();   // never destroyed: it may outlive the CUDA runtime at exit
+  return *c;
+}
+
 struct DevAlloc {
-  std::vector<void *> ptrs;
+  struct Block {
+    void *p;
+    size_t b;
+  };
+  std::vector<Block> blocks;
   uint64_t bytes = 0;
+  int dev = -1;
   template <typename U>
   int alloc(U **p, size_t count)
   {
-    size_t b = sizeof(U) * (count ? count : 1);
-    cudaError_t e = cudaMalloc((void **)p, b);
-    if (e != cudaSuccess) return set_err(VGPU_ENOMEM, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
-    ptrs.push_back(*p);
-    bytes += b;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return set_err(VGPU_ENODEV, "no CUDA device");
+    const size_t b = (sizeof(U) * (count ? count : 1) + 255) / 256 * 256;
+    size_t got = b;
+    void *q = block_cache().take(dev, b, &got);
+    if (!q) {
+      cudaError_t e = cudaMalloc(&q, b);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        block_cache().release(dev);
+        e = cudaMalloc(&q, b);
+      }
+      if (e != cudaSuccess) return set_err(VGPU_ENOMEM, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
+    }
+    *p = (U *)q;
+    blocks.push_back(Block{ q, got });
+    bytes += got;
     return 0;
   }
   void free_all()
   {
-    for (void *p : ptrs) cudaFree(p);
-    ptrs.clear();
+    for (const Block &bl : blocks) block_cache().give(dev, bl.b, bl.p);
+    blocks.clear();
   }
 };
 
@@ -601,68 +670,90 @@ struct Engine : EngineBase {
   {
     const TfsfView &tv = efield ? L.te : L.th;
     TfsfList<T> &tl = efield ? L.le : L.lh;
-    struct Ent {
-      int64_t x;
-      int c, q, axis, gi;
-      int s[3];
-      int64_t hq;
+    // A point belongs to the first item (in face order) that holds it; the
+    // later items of the same component that hold it follow it in its run.
+    // Items are enumerated on separate host threads and joined in item order.
+    struct Part {
+      std::vector<TfsfEntry<T>> single, multi;
+      std::vector<int> spos, mpos, mstart;   // mstart: run starts within multi
     };
-    std::vector<Ent> ents;
-    for (int q = 0; q < tv.n; q++) {
+    std::vector<Part> parts(tv.n);
+    auto make = [&](int q, int i, int j, int k, std::vector<TfsfEntry<T>> &ent, std::vector<int> &pos) {
       const TfsfItem &it = tv.it[q];
+      TfsfEntry<T> d;
+      memset(&d, 0, sizeof d);
+      const int64_t hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
+      const int gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
+      d.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
+      d.q = q;
+      d.idv = (T)(efield ? p.idh[it.axis][gi] : p.ide[it.axis][gi]);
+      d.ca = efield ? (T)p.coef[it.c][hq] : (T)0;
+      d.cb = efield ? (T)p.coef[3 + it.c][hq] : (T)p.coef[6 + it.c - HX][hq];
+      ent.push_back(d);
+      int sp[3] = { i, j, k };
+      sp[it.axis] += it.shift;
+      pos.insert(pos.end(), sp, sp + 3);
+    };
+    auto enumerate = [&](int q) {
+      const TfsfItem &it = tv.it[q];
+      Part &pt = parts[q];
+      // Other items of the component that meet this one.
+      int others[12], no = 0;
+      for (int e = 0; e < tv.n; e++)
+        if (e != q && tv.it[e].c == it.c && boxes_meet(tv.it[e].b, it.b)) others[no++] = e;
+      pt.single.reserve(it.b.count());
+      pt.spos.reserve(3 * it.b.count());
       for (int i = it.b.i0; i <= it.b.i1; i++)
         for (int j = it.b.j0; j <= it.b.j1; j++)
           for (int k = it.b.k0; k <= it.b.k1; k++) {
-            Ent e;
-            e.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
-            e.c = it.c;
-            e.q = q;
-            e.axis = it.axis;
-            e.gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
-            e.s[0] = i; e.s[1] = j; e.s[2] = k;
-            e.s[it.axis] += it.shift;
-            e.hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
-            ents.push_back(e);
+            bool owned = true, followers = false;
+            for (int o = 0; o < no && owned; o++) {
+              if (!tv.it[others[o]].b.contains(i, j, k)) continue;
+              if (others[o] < q) owned = false;
+              else followers = true;
+            }
+            if (!owned) continue;
+            if (!followers) {
+              make(q, i, j, k, pt.single, pt.spos);
+              continue;
+            }
+            pt.mstart.push_back((int)pt.multi.size());
+            make(q, i, j, k, pt.multi, pt.mpos);
+            for (int o = 0; o < no; o++)
+              if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.multi, pt.mpos);
           }
+    };
+    {
+      std::vector<std::thread> pool;
+      for (int q = 1; q < tv.n; q++) pool.emplace_back(enumerate, q);
+      if (tv.n > 0) enumerate(0);
+      for (auto &t : pool) t.join();
     }
-    std::stable_sort(ents.begin(), ents.end(), [](const Ent &a, const Ent &b) {
-      return a.c != b.c ? a.c < b.c : a.x < b.x;
-    });
     // Points of one entry first, then the multi-entry points' runs.
-    const size_t ne = ents.size();
-    std::vector<size_t> order;
-    std::vector<int> mstart;
-    order.reserve(ne);
-    std::vector<std::pair<size_t, size_t>> runs;
-    for (size_t e = 0; e < ne;) {
-      size_t f = e + 1;
-      while (f < ne && ents[f].x == ents[e].x && ents[f].c == ents[e].c) f++;
-      if (f - e == 1) order.push_back(e);
-      else runs.push_back({ e, f });
-      e = f;
+    size_t ns = 0, nm = 0;
+    for (const Part &pt : parts) {
+      ns += pt.single.size();
+      nm += pt.multi.size();
     }
-    const int nsingle = (int)order.size();
-    for (auto &r : runs) {
-      mstart.push_back((int)order.size());
-      for (size_t e = r.first; e < r.second; e++) order.push_back(e);
+    const size_t ne = ns + nm;
+    std::vector<TfsfEntry<T>> ent;
+    std::vector<int> pos, mstart;
+    ent.reserve(ne);
+    pos.reserve(3 * ne);
+    for (const Part &pt : parts) {
+      ent.insert(ent.end(), pt.single.begin(), pt.single.end());
+      pos.insert(pos.end(), pt.spos.begin(), pt.spos.end());
     }
-    mstart.push_back((int)order.size());
-    std::vector<TfsfEntry<T>> ent(ne);
-    std::vector<int> pos(3 * ne);
-    for (size_t o = 0; o < ne; o++) {
-      const Ent &en = ents[order[o]];
-      TfsfEntry<T> &d = ent[o];
-      memset(&d, 0, sizeof d);
-      d.x = en.x;
-      d.q = en.q;
-      d.idv = (T)(efield ? p.idh[en.axis][en.gi] : p.ide[en.axis][en.gi]);
-      d.ca = efield ? (T)p.coef[en.c][en.hq] : (T)0;
-      d.cb = efield ? (T)p.coef[3 + en.c][en.hq] : (T)p.coef[6 + en.c - HX][en.hq];
-      for (int a = 0; a < 3; a++) pos[3 * o + a] = en.s[a];
+    for (const Part &pt : parts) {
+      const int base = (int)ent.size();
+      for (int m : pt.mstart) mstart.push_back(base + m);
+      ent.insert(ent.end(), pt.multi.begin(), pt.multi.end());
+      pos.insert(pos.end(), pt.mpos.begin(), pt.mpos.end());
     }
+    mstart.push_back((int)ne);
     tl.nentries = (int64_t)ne;
-    tl.nsingle = nsingle;
-    tl.nmulti = (int)runs.size();
+    tl.nsingle = (int)ns;
+    tl.nmulti = (int)mstart.size() - 1;
     if (!ne) return 0;
     TfsfEntry<T> *de;
     int *dpos, *dm;
@@ -678,49 +769,94 @@ struct Engine : EngineBase {
   }
 
   // Distinct coefficient tuples per cell: (alpha, beta) x 3 for E and
-  // gamma x 3 for H.  Up to 256 tuples compress to one byte per cell.
+  // gamma x 3 for H.  Up to 256 tuples compress to one byte per cell.  The
+  // i planes are split among host threads; each numbers the tuples it meets,
+  // and the tables merge in plane order, so the numbering does not depend on
+  // the thread count.
   int build_index(int first, int count, CoefIndex &out)
   {
     out = CoefIndex{};
-    std::vector<T> table;
-    std::vector<uint8_t> idx((size_t)vol, 0);
     struct Key {
       T v[6];
       bool operator<(const Key &o) const { return memcmp(v, o.v, sizeof v) < 0; }
     };
-    std::map<Key, int> seen;
-    int last = -1;
-    Key lastk{};
-    for (int i = 0; i < p.n[0]; i++)
-      for (int j = 0; j < p.n[1]; j++)
-        for (int k = 0; k < p.n[2]; k++) {
-          int64_t hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
-          Key key{};
-          for (int c = 0; c < count; c++) key.v[c] = (T)p.coef[first + c][hq];
-          int q = -1;
-          if (last >= 0 && memcmp(key.v, lastk.v, sizeof key.v) == 0) q = last;
-          if (q < 0) {
-            auto it = seen.find(key);
-            if (it != seen.end()) q = it->second;
+    const int n0 = p.n[0];
+    const int nthr = std::max(1, std::min<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())), n0));
+    std::vector<uint8_t> idx((size_t)vol, 0);
+    struct Part {
+      std::vector<Key> keys;   // local tuples in first-seen order
+      bool overflow = false;
+    };
+    std::vector<Part> parts(nthr);
+    auto work = [&](int w) {
+      const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
+      Part &pt = parts[w];
+      std::map<Key, int> seen;
+      int last = -1;
+      Key lastk{};
+      for (int i = i0; i < i1 && !pt.overflow; i++)
+        for (int j = 0; j < p.n[1]; j++) {
+          const int64_t hrow = ((int64_t)i * p.n[1] + j) * p.n[2];
+          uint8_t *irow = idx.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
+          for (int k = 0; k < p.n[2]; k++) {
+            Key key{};
+            for (int c = 0; c < count; c++) key.v[c] = (T)p.coef[first + c][hrow + k];
+            int q = -1;
+            if (last >= 0 && memcmp(key.v, lastk.v, sizeof key.v) == 0) q = last;
+            if (q < 0) {
+              auto it = seen.find(key);
+              if (it != seen.end()) q = it->second;
+            }
+            if (q < 0) {
+              if (seen.size() == 256) {
+                pt.overflow = true;
+                return;
+              }
+              q = (int)seen.size();
+              seen.emplace(key, q);
+              pt.keys.push_back(key);
+            }
+            last = q;
+            lastk = key;
+            irow[k] = (uint8_t)q;
           }
-          if (q < 0) {
-            if (seen.size() == 256) return 0;  // too many: keep the full volumes
-            q = (int)seen.size();
-            seen.emplace(key, q);
-            for (int c = 0; c < count; c++) table.push_back(key.v[c]);
-          }
-          last = q;
-          lastk = key;
-          idx[(int64_t)i * g.s0 + (int64_t)j * g.s1 + k] = (uint8_t)q;
         }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nthr; w++) pool.emplace_back(work, w);
+    work(0);
+    for (auto &t : pool) t.join();
+    // Merge: global numbers in plane order, then renumber each part's planes.
+    std::map<Key, int> global;
+    std::vector<T> table;
+    for (int w = 0; w < nthr; w++) {
+      if (parts[w].overflow) return 0;  // too many: keep the full volumes
+      uint8_t remap[256];
+      for (size_t q = 0; q < parts[w].keys.size(); q++) {
+        const Key &key = parts[w].keys[q];
+        auto it = global.find(key);
+        if (it == global.end()) {
+          if (global.size() == 256) return 0;
+          it = global.emplace(key, (int)global.size()).first;
+          for (int c = 0; c < count; c++) table.push_back(key.v[c]);
+        }
+        remap[q] = (uint8_t)it->second;
+      }
+      bool ident = true;
+      for (size_t q = 0; q < parts[w].keys.size(); q++) ident = ident && remap[q] == q;
+      if (ident) continue;
+      const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
+      for (int64_t x = (int64_t)i0 * g.s0; x < (int64_t)i1 * g.s0; x++) idx[x] = remap[idx[x]];
+    }
     uint8_t *d_idx;
     T *d_tab;
     if (upload(&d_idx, idx.data(), idx.size()) || upload(&d_tab, table.data(), table.size())) return VGPU_ENOMEM;
     out.idx = d_idx;
     out.table = d_tab;
-    out.ntab = (int)seen.size();
+    out.ntab = (int)global.size();
     return 0;
   }
+
 
   // ---- TMA sweeps ------------------------------------------------------
 
