@@ -244,6 +244,8 @@ struct Engine : EngineBase {
   PmlFull<T> pfe{}, pfh{};
   int pml_face[6] = {};
   int *d_err = nullptr;
+  cudaStream_t s2 = nullptr;                   // second stream of the sweep pairs
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // fused sweeps
   CoefIndex cie{}, cih{};
   // graph
@@ -254,6 +256,7 @@ struct Engine : EngineBase {
   {
     if (graph) cudaGraphExecDestroy(graph);
     if (s) cudaStreamSynchronize(s);
+    if (s2) cudaStreamSynchronize(s2);
     if (cs) cudaStreamSynchronize(cs);
     mem.free_all();
     if (h_bin) cudaFreeHost(h_bin);
@@ -261,7 +264,10 @@ struct Engine : EngineBase {
       if (ev_fill[q]) cudaEventDestroy(ev_fill[q]);
       if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
     }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (cs) cudaStreamDestroy(cs);
+    if (s2) cudaStreamDestroy(s2);
     if (s) cudaStreamDestroy(s);
   }
 
@@ -302,6 +308,9 @@ struct Engine : EngineBase {
   {
     p = *in;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     n2p = (p.n[2] + 31) / 32 * 32;
     g.n0 = p.n[0];
     g.n1 = p.n[1];
@@ -1149,8 +1158,9 @@ struct Engine : EngineBase {
 
   // Launch one sweep kernel of a half step: which = 0 the bulk tiles, 1 the
   // UPML and mixed tiles.  Counts launched kernels through `count`.
-  int launch_sweeps(bool esweep, int which, uint64_t *count)
+  int launch_sweeps(bool esweep, int which, uint64_t *count, cudaStream_t st = nullptr)
   {
+    if (!st) st = s;
     const dim3 blk(kSweepThreads);
     SweepLaunch &L = (esweep ? sw_e : sw_h)[which];
     if (!L.ntiles) return 0;
@@ -1158,16 +1168,16 @@ struct Engine : EngineBase {
     const PmlFull<T> &pf = esweep ? pfe : pfh;
     const SweepMaps &mp = esweep ? maps_e : maps_h;
     if (esweep && which == 0)
-      k_sweep_tma<T, true, false><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
+      k_sweep_tma<T, true, false><<<L.grid, blk, L.smem, st>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
                                                             L.ntiles, pf, ci, d_err);
     else if (esweep)
-      k_sweep_tma<T, true, true><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
+      k_sweep_tma<T, true, true><<<L.grid, blk, L.smem, st>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
                                                            L.ntiles, pf, ci, d_err);
     else if (which == 0)
-      k_sweep_tma<T, false, false><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
+      k_sweep_tma<T, false, false><<<L.grid, blk, L.smem, st>>>(mp, g, L.tiles, (const SweepHeader<T, false> *)L.headers,
                                                              L.ntiles, pf, ci, d_err);
     else
-      k_sweep_tma<T, false, true><<<L.grid, blk, L.smem, s>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
+      k_sweep_tma<T, false, true><<<L.grid, blk, L.smem, st>>>(mp, g, L.tiles, (const SweepHeader<T, true> *)L.headers,
                                                             L.ntiles, pf, ci, d_err);
     if (count) ++*count;
     return 0;
@@ -1274,6 +1284,25 @@ struct Engine : EngineBase {
 
   static unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
+  // The bulk and UPML sweeps of a half step write disjoint points and read
+  // only the other field, so they run side by side: the UPML launch on a
+  // second stream, forked from and joined back to the engine's stream.
+  int launch_sweep_pair(bool esweep, uint64_t *count)
+  {
+    const SweepLaunch *L = esweep ? sw_e : sw_h;
+    if (!L[0].ntiles || !L[1].ntiles) {
+      if (int rc = launch_sweeps(esweep, 1, count)) return rc;
+      return launch_sweeps(esweep, 0, count);
+    }
+    CK(cudaEventRecord(ev_fork, s));
+    CK(cudaStreamWaitEvent(s2, ev_fork, 0));
+    if (int rc = launch_sweeps(esweep, 1, count, s2)) return rc;
+    if (int rc = launch_sweeps(esweep, 0, count, s)) return rc;
+    CK(cudaEventRecord(ev_join, s2));
+    CK(cudaStreamWaitEvent(s, ev_join, 0));
+    return 0;
+  }
+
   // One time step, in the order of src/simulation.c:156-222, `rel` steps
   // past the device step counter.
   int enqueue_step(int rel)
@@ -1294,8 +1323,7 @@ struct Engine : EngineBase {
     // Mur reads the neighbours' pre-update E, so it precedes the sweeps; the
     // PML and bulk sweeps touch disjoint E points.
     if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
-    if (int rc = launch_one(VGPU_K_PML_E, false, &launches)) return rc;
-    if (int rc = launch_one(VGPU_K_BULK_E, false, &launches)) return rc;
+    if (int rc = launch_sweep_pair(true, &launches)) return rc;
     if (n_debye) {
       k_debye<T><<<blocks_for(debye_total, 128), 128, 0, s>>>(g, d_debye, n_debye, debye_total, d_J, d_lastE, d_dcoef);
       launches++;
@@ -1322,8 +1350,7 @@ struct Engine : EngineBase {
       launches++;
     }
     if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
-    if (int rc = launch_one(VGPU_K_PML_H, false, &launches)) return rc;
-    if (int rc = launch_one(VGPU_K_BULK_H, false, &launches)) return rc;
+    if (int rc = launch_sweep_pair(false, &launches)) return rc;
     if (nsibc && ntgt) {
       k_sibc_h<T><<<blocks_for(ntgt, 128), 128, 0, s>>>(g, d_tgt_index, d_tgt_comp, d_tgt_start, ntgt, d_ops, d_etan);
       launches++;
