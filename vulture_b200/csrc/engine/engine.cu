@@ -694,7 +694,7 @@ struct Engine : EngineBase {
       const int64_t hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
       const int gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
       d.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
-      d.q = q;
+      d.meta = q;
       d.idv = (T)(efield ? p.idh[it.axis][gi] : p.ide[it.axis][gi]);
       d.ca = efield ? (T)p.coef[it.c][hq] : (T)0;
       d.cb = efield ? (T)p.coef[3 + it.c][hq] : (T)p.coef[6 + it.c - HX][hq];

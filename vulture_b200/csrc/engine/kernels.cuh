@@ -535,12 +535,12 @@ __global__ void k_aux_h(PwView<T> pw)
 template <typename T>
 struct alignas(16) TfsfEntry {
   int64_t x;    // field index of the corrected point
-  double dv;    // analytic field: d / phase velocity
+  double dv;    // analytic field: d / phase velocity; auxiliary grid: the fraction
   T idv;        // line length
   T ca, cb;     // alpha and beta (E) or -, gamma (H)
-  T frac;       // auxiliary grid: fraction
-  int cell;     // auxiliary grid: cell
-  int q;        // item (face, component)
+  int meta;     // item (face, component) in bits 0-7; auxiliary-grid cell above
+  __host__ __device__ int q() const { return meta & 255; }
+  __host__ __device__ int cell() const { return meta >> 8; }
 };
 
 template <typename T>
@@ -558,7 +558,7 @@ __global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= tl.nentries) return;
   TfsfEntry<T> &en = tl.ent[e];
-  const int c = tv.it[en.q].inc;
+  const int c = tv.it[en.q()].inc;
   const int i = tl.pos[3 * e], j = tl.pos[3 * e + 1], k = tl.pos[3 * e + 2];
   if (!pw.use_aux) {
     // Phase term of the analytic incident field (src/planewave.c:450-554):
@@ -580,15 +580,18 @@ __global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
       if (a != c - HX) rc[a] = rc[a] + (T)0.5;
   T d = (T)pw.kinc[0] * (rc[0] - (T)pw.ijk0[0]) + (T)pw.kinc[1] * (rc[1] - (T)pw.ijk0[1]) +
         (T)pw.kinc[2] * (rc[2] - (T)pw.ijk0[2]);
+  // The fraction is a T; stored as a double it round-trips exactly.
+  int id;
+  T frac;
   if (c <= EZ) {
-    int id = (int)floor((double)d);
-    en.cell = id;
-    en.frac = d - (T)id;
+    id = (int)floor((double)d);
+    frac = d - (T)id;
   } else {
-    int id = (int)floor((double)d + 0.5);
-    en.cell = id;
-    en.frac = (T)((double)d + 0.5 - id);
+    id = (int)floor((double)d + 0.5);
+    frac = (T)((double)d + 0.5 - id);
   }
+  en.meta = (en.meta & 255) | (int)((unsigned)id << 8);
+  en.dv = (double)frac;
 }
 
 // One correction of `v` (src/planewave.c:576-1007, the expression of the
@@ -597,13 +600,13 @@ template <typename T>
 __device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv, const TfsfEntry<T> &en, T v,
                                         double time, int efield)
 {
-  const TfsfItem &it = tv.it[en.q];
+  const TfsfItem &it = tv.it[en.q()];
   T inc;
   if (!pw.use_aux) {
     inc = (T)(pw.finc[it.inc] * dev_waveform(pw.wf, time - en.dv, pw.delay));
   } else {
-    const int id = en.cell;
-    const T dp = en.frac;
+    const int id = en.cell();
+    const T dp = (T)en.dv;
     T value;
     if (it.inc <= EZ) value = (1 - dp) * pw.Eyi[2 + id] + dp * pw.Eyi[2 + id + 1];
     else value = pw.eta0 * ((1 - dp) * pw.Hzi[2 - 1 + id] + dp * pw.Hzi[2 + id]);
@@ -627,13 +630,13 @@ __global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl
   const double time = efield ? n * dt : (n + 0.5) * dt;
   if (t < tl.nsingle) {
     const TfsfEntry<T> en = tl.ent[t];
-    T *F = g.F[tv.it[en.q].c];
+    T *F = g.F[tv.it[en.q()].c];
     F[en.x] = tfsf_apply(pw, tv, en, F[en.x], time, efield);
     return;
   }
   const int e0 = tl.mstart[t - tl.nsingle], e1 = tl.mstart[t - tl.nsingle + 1];
   const TfsfEntry<T> first = tl.ent[e0];
-  T *F = g.F[tv.it[first.q].c];
+  T *F = g.F[tv.it[first.q()].c];
   T v = F[first.x];
   for (int e = e0; e < e1; e++) v = tfsf_apply(pw, tv, tl.ent[e], v, time, efield);
   F[first.x] = v;
