@@ -170,6 +170,38 @@ def run_reference_arm(args):
     print(json.dumps(base))
 
 
+def error_report(td, re, im, td64, re64, im64, steps):
+    """FP32 against FP64 on the same steps: time-domain relative L2 per point
+    observer, and the frequency-domain magnitude error in dB per result
+    (observer point and component) over the frequencies whose FP64 magnitude
+    is within 60 dB of that result's peak."""
+    import numpy as np
+
+    a, b = td[:steps], td64[:steps]
+    td_err = []
+    for q in range(b.shape[1]):
+        den = np.sqrt((b[:, q, :] ** 2).sum())
+        if den > 0:
+            td_err.append(float(np.sqrt(((a[:, q, :] - b[:, q, :]) ** 2).sum()) / den))
+    mag = np.hypot(re, im)
+    mag64 = np.hypot(re64, im64)
+    db = []
+    for q in range(mag64.shape[0]):
+        for c in range(6):
+            ref = mag64[q, c]
+            peak = ref.max()
+            if peak <= 0:
+                continue
+            sel = ref > peak * 1e-3
+            d = np.abs(20 * np.log10(np.maximum(mag[q, c][sel], 1e-300)) - 20 * np.log10(ref[sel]))
+            db.append(float(d.max()))
+    db = np.array(db) if db else np.zeros(1)
+    return {"steps": steps, "td_rel_l2_max": max(td_err) if td_err else 0.0, "td_bound": 1e-4,
+            "td_points": len(td_err), "fd_db_max": float(db.max()), "fd_db_median": float(np.median(db)),
+            "fd_db_p99": float(np.percentile(db, 99)), "fd_results": int(db.size),
+            "fd_share_within_1e-3_db": float((db <= 1e-3).mean()), "fd_bound_db": 1e-3}
+
+
 def run_gpu_arm(args):
     import numpy as np
     import torch
@@ -250,15 +282,24 @@ def run_gpu_arm(args):
     e2e_value = world * n_out * args.steps / e2e_wall / 1e6
     d2h = td.nbytes + re.nbytes + im.nbytes
 
-    # Plain FP64 on the same workload, for the FP32-vs-FP64 comparison.
+    # Plain FP64 on the same workload and steps: its throughput, and the FP32
+    # run's error against it, per result (time-domain relative L2 per point
+    # observer; frequency-domain magnitude in dB over the frequencies within
+    # 60 dB of each result's peak).
     fp64 = None
+    fp32_error = None
     if prec == "fp32" and not args.no_fp64:
         g3 = vb.GpuRun(m, "fp64")
-        g3.run(args.warmup)
-        g3.run(min(args.steps, 400))
+        w64 = min(args.warmup, args.steps - 1) if args.steps > 1 else 0
+        if w64:
+            g3.run(w64)
+        g3.run(args.steps - w64)
         st3 = g3.stats()
         fp64 = n_out * st3.steps / (st3.run_ms * 1e-3) / 1e6
+        td64 = g3.td(args.steps)
+        re64, im64 = g3.dft()
         g3.close()
+        fp32_error = error_report(td, re, im, td64, re64, im64, args.steps)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -298,12 +339,160 @@ def run_gpu_arm(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "fp64_value": fp64,
+            "fp32_error": fp32_error,
             "cpu_baseline": cpu,
         }
         print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _meshes_dir(texts, prefix):
+    from vulture_b200 import meshgen
+
+    d = Path(tempfile.mkdtemp(prefix=prefix))
+    return d, [meshgen.write(t, d / f"m{q:03d}.mesh") for q, t in enumerate(texts)]
+
+
+def _sweep_bytes(g, prec):
+    """Algorithmic bytes of one step of an engine: the four sweeps' points by
+    the bulk or UPML word count."""
+    from vulture_b200 import _native as N
+
+    tot = 0.0
+    for kid, wb, wp in ((N.VGPU_K_BULK_E, WORDS_E, WORDS_PML_E), (N.VGPU_K_BULK_H, WORDS_H, WORDS_PML_H),
+                        (N.VGPU_K_PML_E, WORDS_E, WORDS_PML_E), (N.VGPU_K_PML_H, WORDS_H, WORDS_PML_H)):
+        bp, pp = g.sweep_points(kid)
+        tot += (wb * bp + wp * pp) / 3.0 * B_ALG[prec]
+    return tot
+
+
+def run_batch_workload(args):
+    """Many independent meshes of uneven size (seeded PEC/dielectric slabs,
+    6-cell UPML, a hard or soft dipole), FP32, advanced together through
+    vgpu_run_batch, against the same meshes solved one after another by the
+    plain FP64 path.  Solves/s counts create + steps + observer read-back."""
+    import torch
+
+    import vulture_b200 as vb
+    from vulture_b200 import meshgen
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    rng = __import__("random").Random(4 + rank)
+    texts = [meshgen.config4_mesh(rng, q, nmin=32, nmax=160, ntmin=args.batch_steps[0], ntmax=args.batch_steps[1])
+             for q in range(args.batch_count)]
+    d, paths = _meshes_dir(texts, "vb_batch_")
+    meshes = [vb.Mesh(p) for p in paths]
+    cell_updates = sum(m.num_cells * m.num_steps for m in meshes)
+    # Warm-up: one small solve of each precision (module load, caches).
+    for prec in ("fp32", "fp64"):
+        vb.GpuRun(meshes[0], prec).run(min(64, meshes[0].num_steps)).close()
+    torch.cuda.synchronize()
+
+    def batch_pass():
+        t0 = time.perf_counter()
+        runs = [vb.GpuRun(m, "fp32") for m in meshes]
+        t1 = time.perf_counter()
+        vb.run_batch(runs)
+        t2 = time.perf_counter()
+        for r in runs:
+            r.td()
+        t3 = time.perf_counter()
+        nbytes = sum(_sweep_bytes(r, "fp32") * r.mesh.num_steps for r in runs)
+        launches = sum(int(r.stats().kernel_launches) for r in runs)
+        for r in runs:
+            r.close()
+        return t3 - t0, t2 - t1, nbytes, launches
+
+    with ClockSampler(local) as clk:
+        wall32, step_s, nbytes, launches = batch_pass()
+    t0 = time.perf_counter()
+    for m in meshes:
+        g = vb.GpuRun(m, "fp64").run()
+        g.td()
+        g.close()
+    wall64 = time.perf_counter() - t0
+    peak, peak_kind = peaks()
+    achieved = nbytes / step_s / 1e9
+    shutil.rmtree(d, ignore_errors=True)
+    sps32, sps64 = len(meshes) / wall32, len(meshes) / wall64
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched solves/s", "value": sps32 * world, "unit": "solves/s", "n_gpus": world,
+            "steps": 1, "warmup": 1, "ms_per_step": wall32 * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"{len(meshes)} meshes, per-axis 32-160 cells, 6-cell UPML, PEC/dielectric "
+                                   f"slabs, dipole; {args.batch_steps[0]}-{args.batch_steps[1]} steps each",
+                       "cell_updates": cell_updates, "batch": "vgpu_run_batch, one stream per engine"},
+            "mcell_updates_per_s": cell_updates / step_s / 1e6,
+            "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
+            "fp64_sequential_solves_per_s": sps64, "speedup_vs_fp64_sequential": sps32 / sps64,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "what": "algorithmic sweep bytes of every engine over the batch's stepping time"},
+            "e2e": {"value": sps32 * world, "unit": "solves/s", "wall_s": wall32, "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None},
+            "gpu_launches": launches, "clocks": clk.summary()}))
+
+
+def run_serve_workload(args):
+    """A seeded Poisson stream of solve requests (lognormal sizes, UPML or
+    Mur, optional Debye block and TFSF source), FP32, served with admission
+    by an HBM budget and continuous batching; the same stream solved one at a
+    time by the plain FP64 path gives the comparison latencies."""
+    import random
+
+    import torch
+
+    import vulture_b200 as vb
+    from vulture_b200 import meshgen
+    from vulture_b200.serve import Request, Server, latency_summary
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    rng = random.Random(5 + rank)
+    texts = [meshgen.config5_request(rng, q, nmin=48, nmax=args.serve_nmax, ntmin=args.serve_steps[0],
+                                     ntmax=args.serve_steps[1]) for q in range(args.serve_count)]
+    arrivals, t = [], 0.0
+    for _ in texts:
+        t += rng.expovariate(args.serve_rate)
+        arrivals.append(t)
+    d, paths = _meshes_dir(texts, "vb_serve_")
+    warm = vb.Mesh(paths[0])
+    for prec in ("fp32", "fp64"):
+        vb.GpuRun(warm, prec).run(min(64, warm.num_steps)).close()
+    torch.cuda.synchronize()
+
+    def serve(prec, budget):
+        reqs = [Request(tx, arrival=a, precision=prec, tag=str(q)) for q, (tx, a) in enumerate(zip(texts, arrivals))]
+        srv = Server(budget)
+        done = srv.run(reqs, keep_results=False)
+        return srv, done
+
+    with ClockSampler(local) as clk:
+        srv, done = serve("fp32", int(args.serve_budget_gb * 2**30))
+    s32 = latency_summary(done)
+    # Plain FP64: the same stream, one solve at a time.
+    srv64, done64 = serve("fp64", 1)
+    s64 = latency_summary(done64)
+    shutil.rmtree(d, ignore_errors=True)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "p99 latency", "value": s32["p99_s"], "unit": "s", "n_gpus": world, "steps": len(done),
+            "warmup": 1, "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"{len(done)} requests, Poisson rate {args.serve_rate}/s, per-axis 48-"
+                                   f"{args.serve_nmax} lognormal, {args.serve_steps[0]}-{args.serve_steps[1]} "
+                                   f"steps, UPML or Mur, Debye, TFSF or dipole",
+                       "budget_gb": args.serve_budget_gb},
+            "fp32": s32, "fp64_one_at_a_time": s64,
+            "p99_ratio_fp64_over_fp32": s64["p99_s"] / s32["p99_s"],
+            "solves_per_s_ratio": s32["solves_per_s"] / s64["solves_per_s"],
+            "peak_active": srv.peak_active, "peak_budget_bytes": srv.peak_bytes,
+            "e2e": {"value": s32["p99_s"], "unit": "s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "clocks": clk.summary()}))
 
 
 def main():
@@ -315,11 +504,23 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="config2", choices=["config2", "batch", "serve"])
+    ap.add_argument("--batch-count", type=int, default=32)
+    ap.add_argument("--batch-steps", type=int, nargs=2, default=[400, 1600])
+    ap.add_argument("--serve-count", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-nmax", type=int, default=128)
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[400, 4000])
+    ap.add_argument("--serve-budget-gb", type=float, default=8.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "batch":
+        run_batch_workload(args)
+    elif args.workload == "serve":
+        run_serve_workload(args)
     else:
         run_gpu_arm(args)
 

@@ -268,6 +268,24 @@ typedef void (*vgpu_bin_sink)(void *user, uint64_t first_row, uint32_t num_rows,
  * every 64-step block to pinned host memory on a second stream. */
 int vgpu_set_bin_sink(vgpu_engine *engine, vgpu_bin_sink sink, void *user);
 
+/* Asynchronous stepping, for callers that keep several engines busy on one
+ * device (batches, services).  vgpu_enqueue queues at most max_steps more
+ * steps -- one 64-step graph, or single steps up to the next 64-step
+ * boundary, never past the problem's last step -- on the engine's stream and
+ * returns without waiting; *queued receives the count (0 once the problem is
+ * done).  Observer folding and binary-row delivery happen as in vgpu_run.
+ * vgpu_query returns 1 when the queued work has finished, 0 if not;
+ * vgpu_synchronize waits for it and reports any device-side failure. */
+int vgpu_enqueue(vgpu_engine *engine, uint64_t max_steps, uint64_t *queued);
+int vgpu_query(vgpu_engine *engine);
+int vgpu_synchronize(vgpu_engine *engine);
+
+/* Advance n engines of one device by steps[i] each: their blocks are queued
+ * round-robin on the engines' own streams, so the device runs them side by
+ * side; returns when all have finished.  The batched form of vgpu_run; each
+ * engine's results are the ones vgpu_run would give it alone. */
+int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint64_t *steps);
+
 /* Copy time-domain samples to the host: out[(s*num_td + p)*6 + c] for the
  * first `steps` steps of the output window. */
 int vgpu_read_td(vgpu_engine *engine, double *out, uint64_t steps);

@@ -83,6 +83,10 @@ def lib() -> C.CDLL:
         "vgpu_get_stats": (C.c_int, [P, C.POINTER(VgpuStats)]),
         "vgpu_set_bin_sink": (C.c_int, [P, P, P]),
         "vgpu_sweep_points": (C.c_int, [P, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vgpu_enqueue": (C.c_int, [P, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "vgpu_query": (C.c_int, [P]),
+        "vgpu_synchronize": (C.c_int, [P]),
+        "vgpu_run_batch": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(C.c_uint64)]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
     }
@@ -111,6 +115,7 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vgpu_read_td", "vgpu_read_dft", "vgpu_read_field", "vgpu_write_field", "vgpu_check_finite",
            "vgpu_current_step", "vgpu_time_kernel", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error",
            "vgpu_set_bin_sink", "vgpu_dft_accumulate_static", "vhost_num_bin", "vhost_bin_begin", "vhost_bin_sink",
-           "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points"]
+           "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
+           "vgpu_synchronize", "vgpu_run_batch"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3

@@ -148,6 +148,10 @@ struct EngineBase {
   virtual int check_finite() = 0;
   virtual int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) = 0;
   virtual int sweep_points(int kernel, uint64_t *bulk_pts, uint64_t *pml_pts) = 0;
+  virtual int check_steps(uint64_t nsteps) = 0;
+  virtual int enqueue(uint64_t max_steps, uint64_t *queued) = 0;
+  virtual int query() = 0;
+  virtual int synchronize() = 0;
   vgpu_bin_sink bin_sink = nullptr;
   void *bin_user = nullptr;
   uint64_t step = 0;
@@ -1410,64 +1414,103 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  int run(uint64_t nsteps) override
+  // Queue the next block of at most max_steps steps (one captured graph, or
+  // single steps up to the next 64-step boundary) on the engine's stream,
+  // with the block's DFT fold and binary-row copy; *queued gets the count.
+  int issue_block(uint64_t max_steps, uint64_t *queued)
   {
-    if (step + nsteps > p.num_steps)
-      return set_err(VGPU_EINVAL, "run of %llu steps from step %llu exceeds the problem's %llu steps",
-                     (unsigned long long)nsteps, (unsigned long long)step, (unsigned long long)p.num_steps);
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, s));
-    uint64_t done = 0, launches = 0;
-    stats.kernel_launches = 0;
-    while (done < nsteps) {
-      uint64_t n0 = step;
-      // Chunks stay aligned so the DFT staging rows of one chunk never wrap.
-      uint64_t room = kChunk - (n0 % kChunk);
-      uint64_t m = std::min<uint64_t>(room, nsteps - done);
-      const int q = (int)((n0 / kChunk) & 1);
-      // The ring block this chunk fills last held the chunk two back: hand
-      // those rows over (the device is busy with the previous chunk) before
-      // they are overwritten.
-      if (p.num_bin > 0)
-        if (int rc = bin_deliver(q)) return rc;
-      if (m == (uint64_t)kChunk) {
-        CK(cudaGraphLaunch(graph, s));
-      } else {
-        if (int rc = enqueue_steps((int)m)) return rc;
-      }
-      launches += m * launches_per_step + 1;
-      step += m;
-      done += m;
-      // Output rows produced in this chunk.
-      uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
-      if (p.num_bin > 0 && bin_sink && hi >= lo && lo <= p.out_stop) {
-        if (int rc = bin_enqueue(q, lo, hi)) return rc;
-      }
-      if (p.num_fd && hi >= lo) {
-        if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
-      }
+    const uint64_t n0 = step;
+    // Blocks stay aligned so the DFT staging rows of one block never wrap.
+    const uint64_t room = kChunk - (n0 % kChunk);
+    const uint64_t m = std::min<uint64_t>(room, max_steps);
+    *queued = 0;
+    if (!m) return 0;
+    const int q = (int)((n0 / kChunk) & 1);
+    // The ring block this chunk fills last held the chunk two back: hand
+    // those rows over (the device is busy with the previous chunk) before
+    // they are overwritten.
+    if (p.num_bin > 0)
+      if (int rc = bin_deliver(q)) return rc;
+    if (m == (uint64_t)kChunk) {
+      CK(cudaGraphLaunch(graph, s));
+    } else {
+      if (int rc = enqueue_steps((int)m)) return rc;
     }
-    CK(cudaEventRecord(e1, s));
-    CK(cudaEventSynchronize(e1));
+    stats.kernel_launches += m * launches_per_step + 1;
+    step += m;
+    // Output rows produced in this block.
+    const uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
+    if (p.num_bin > 0 && bin_sink && hi >= lo && lo <= p.out_stop) {
+      if (int rc = bin_enqueue(q, lo, hi)) return rc;
+    }
+    if (p.num_fd && hi >= lo) {
+      if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
+    }
+    *queued = m;
+    return 0;
+  }
+
+  // After the queued work has finished: errors, then the binary rows still
+  // pending, older block first.
+  int finish_queued()
+  {
     if (int rc = check_device_error()) return rc;
     if (p.num_bin > 0) {
-      // The older pending block first.
       int a = 0, b = 1;
       if (bin_blk[1].pending && (!bin_blk[0].pending || bin_blk[1].row0 < bin_blk[0].row0)) a = 1, b = 0;
       if (int rc = bin_deliver(a)) return rc;
       if (int rc = bin_deliver(b)) return rc;
     }
     CK(cudaGetLastError());
+    return 0;
+  }
+
+  int check_steps(uint64_t nsteps) override
+  {
+    if (step + nsteps > p.num_steps)
+      return set_err(VGPU_EINVAL, "run of %llu steps from step %llu exceeds the problem's %llu steps",
+                     (unsigned long long)nsteps, (unsigned long long)step, (unsigned long long)p.num_steps);
+    return 0;
+  }
+
+  int run(uint64_t nsteps) override
+  {
+    if (int rc = check_steps(nsteps)) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+    stats.kernel_launches = 0;
+    for (uint64_t done = 0; done < nsteps;) {
+      uint64_t m = 0;
+      if (int rc = issue_block(nsteps - done, &m)) return rc;
+      done += m;
+    }
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    if (int rc = finish_queued()) return rc;
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     stats.run_ms = ms;
     stats.steps = nsteps;
-    stats.kernel_launches += launches;
     return 0;
+  }
+
+  // Up to max_steps more steps, never past the problem's last step.
+  int enqueue(uint64_t max_steps, uint64_t *queued) override
+  {
+    const uint64_t left = step < p.num_steps ? p.num_steps - step : 0;
+    return issue_block(std::min<uint64_t>(max_steps, left), queued);
+  }
+
+  int query() override { return cudaStreamQuery(s) == cudaSuccess ? 1 : 0; }
+
+  int synchronize() override
+  {
+    CK(cudaStreamSynchronize(s));
+    return finish_queued();
   }
 
   int read_td(double *out, uint64_t steps) override
@@ -1686,6 +1729,52 @@ extern "C" int vgpu_check_finite(vgpu_engine *e)
 }
 
 extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
+
+extern "C" int vgpu_enqueue(vgpu_engine *e, uint64_t max_steps, uint64_t *queued)
+{
+  if (!e || !queued) return set_err(VGPU_EINVAL, "null argument");
+  return e->impl->enqueue(max_steps, queued);
+}
+
+extern "C" int vgpu_query(vgpu_engine *e)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  return e->impl->query();
+}
+
+extern "C" int vgpu_synchronize(vgpu_engine *e)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  return e->impl->synchronize();
+}
+
+extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint64_t *steps)
+{
+  if (n < 0 || (n && (!engines || !steps))) return set_err(VGPU_EINVAL, "invalid batch");
+  for (int32_t i = 0; i < n; i++) {
+    if (!engines[i]) return set_err(VGPU_EINVAL, "null engine %d in batch", (int)i);
+    if (int rc = engines[i]->impl->check_steps(steps[i])) return rc;
+  }
+  std::vector<uint64_t> left(steps, steps + n);
+  for (bool any = true; any;) {
+    any = false;
+    for (int32_t i = 0; i < n; i++) {
+      if (!left[i]) continue;
+      uint64_t m = 0;
+      if (int rc = engines[i]->impl->enqueue(left[i], &m)) return rc;
+      // An engine listed twice can reach its last step before its count.
+      if (!m) return set_err(VGPU_EINVAL, "engine %d in batch reached its last step", (int)i);
+      left[i] -= m;
+      any = any || left[i] > 0;
+    }
+  }
+  int rc = 0;
+  for (int32_t i = 0; i < n; i++) {
+    int r = engines[i]->impl->synchronize();
+    if (r && !rc) rc = r;
+  }
+  return rc;
+}
 
 extern "C" int vgpu_sweep_points(const vgpu_engine *e, int32_t kernel, uint64_t *bulk_points, uint64_t *pml_points)
 {

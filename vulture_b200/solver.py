@@ -181,6 +181,21 @@ class GpuRun:
     def step(self) -> int:
         return int(N.lib().vgpu_current_step(self._e))
 
+    def enqueue(self, max_steps: int = 64) -> int:
+        """Queue up to max_steps more steps (one 64-step block at most) without
+        waiting; returns the steps queued, 0 once the problem is done."""
+        q = C.c_uint64()
+        N.check_gpu(N.lib().vgpu_enqueue(self._e, max_steps, C.byref(q)))
+        return q.value
+
+    def done(self) -> bool:
+        """True when the queued steps have finished on the device."""
+        return N.lib().vgpu_query(self._e) == 1
+
+    def synchronize(self):
+        N.check_gpu(N.lib().vgpu_synchronize(self._e))
+        return self
+
     def stats(self) -> N.VgpuStats:
         st = N.VgpuStats()
         N.check_gpu(N.lib().vgpu_get_stats(self._e, C.byref(st)))
@@ -237,6 +252,18 @@ class GpuRun:
             self.close()
         except Exception:
             pass
+
+
+def run_batch(runs, steps=None):
+    """Advance several GpuRun engines of one device together (vgpu_run_batch):
+    steps[i] more steps each (default: to the end of each problem)."""
+    n = len(runs)
+    if steps is None:
+        steps = [r.mesh.num_steps - r.step for r in runs]
+    arr = (C.c_void_p * n)(*[r._e.value for r in runs])
+    st = (C.c_uint64 * n)(*steps)
+    N.check_gpu(N.lib().vgpu_run_batch(arr, n, st))
+    return runs
 
 
 def run_mesh(mesh_path, out_dir, precision="fp64", full_precision=False):
