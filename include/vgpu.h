@@ -244,8 +244,15 @@ typedef struct {
 
 /* Create an engine on the current CUDA device (cuda:0 unless the caller set
  * another) and upload the problem.  Replaces the state the reference builds
- * in src/vulture.c:95-148 before propagate(). */
+ * in src/vulture.c:95-148 before propagate().  An engine may be driven from
+ * any host thread: each entry point that takes it makes its device current
+ * on the calling thread first.  Calls on one engine must not overlap. */
 int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
+
+/* The calling thread's current CUDA device, for hosts without the CUDA
+ * runtime of their own (worker threads that create engines for a device). */
+int vgpu_set_device(int32_t device);
+int vgpu_get_device(int32_t *device);
 
 /* Advance nsteps time steps (the loop body of src/simulation.c:156-222),
  * continuing from the engine's current step.  Returns once the device has

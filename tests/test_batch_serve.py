@@ -12,7 +12,7 @@ import pytest
 
 import vulture_b200 as vb
 from vulture_b200 import meshgen
-from vulture_b200.serve import Request, Server, footprint_estimate, latency_summary
+from vulture_b200.serve import Request, Server, footprint_estimate, latency_summary, solve_batch
 from helpers import stage_text
 
 pytestmark = pytest.mark.gpu
@@ -50,6 +50,15 @@ def test_batch_equals_solo(precision):
     runs = [vb.GpuRun(m, precision) for m in meshes]
     runs[1].run(17)          # one engine starts mid-block
     vb.run_batch(runs)
+    for m, a, b in zip(meshes, runs, solo):
+        assert a.step == m.num_steps
+        assert_same_run(m, a, b)
+
+
+def test_solve_batch_equals_solo():
+    meshes = [vb.Mesh(p) for p in small_meshes()]
+    solo = [vb.GpuRun(m, "fp32").run() for m in meshes]
+    runs = solve_batch(meshes, "fp32", workers=2)
     for m, a, b in zip(meshes, runs, solo):
         assert a.step == m.num_steps
         assert_same_run(m, a, b)

@@ -68,7 +68,7 @@ def build_engine(verbose: bool = False) -> Path:
                 print(out)
         objs.append(o)
     if _stale(LIB, objs):
-        _run([NVCC, *GENCODE, "-shared", "-o", LIB, *objs, "-lm"])
+        _run([NVCC, *GENCODE, "-shared", "-o", LIB, *objs, "-lm", "-lpthread"])
     if _stale(CLI, [LIB, PKG / "csrc" / "cli_main.c"]):
         CLI.parent.mkdir(parents=True, exist_ok=True)
         _run(["gcc", "-O2", f"-I{ROOT / 'include'}", PKG / "csrc" / "cli_main.c", "-o", CLI,

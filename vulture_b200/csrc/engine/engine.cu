@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <thread>
@@ -43,8 +44,9 @@ extern "C" const char *vgpu_last_error(void) { return g_err; }
     if (e_ != cudaSuccess) return set_err(VGPU_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
-static const int kChunk = 64;      // steps per captured graph and per DFT block
+static const int kChunk = 64;      // steps per block and per DFT block
 static const int kTB = kChunk;     // DFT staging rows
+static const int kGraphSteps = 16; // steps per captured graph; a block launches it kChunk / kGraphSteps times
 
 // The device step counter moves once per block of steps; kernels inside
 // the block add their step's offset (step_rel).
@@ -74,13 +76,17 @@ struct BlockCache {
     fb.erase(it);
     return p;
   }
-  void give(int dev, size_t b, void *p)
+  // Takes back n blocks; past a quarter of the device's memory the cache
+  // is released.
+  void give(int dev, size_t n, const size_t *b, void *const *p)
   {
     std::lock_guard<std::mutex> lk(mu);
     size_t total = 0, fr = 0;
     cudaMemGetInfo(&fr, &total);
-    free_blocks[dev].emplace(b, p);
-    held[dev] += b;
+    for (size_t q = 0; q < n; q++) {
+      free_blocks[dev].emplace(b[q], p[q]);
+      held[dev] += b[q];
+    }
     if (held[dev] > total / 4) release_locked(dev);
   }
   void release(int dev)
@@ -133,7 +139,13 @@ struct DevAlloc {
   }
   void free_all()
   {
-    for (const Block &bl : blocks) block_cache().give(dev, bl.b, bl.p);
+    std::vector<size_t> b;
+    std::vector<void *> q;
+    for (const Block &bl : blocks) {
+      b.push_back(bl.b);
+      q.push_back(bl.p);
+    }
+    if (!blocks.empty()) block_cache().give(dev, b.size(), b.data(), q.data());
     blocks.clear();
   }
 };
@@ -308,7 +320,35 @@ struct Engine : EngineBase {
     return 0;
   }
 
+  // With VGPU_TRACE set, create() prints the time of each set-up phase.
+  struct PhaseClock {
+    bool on = getenv("VGPU_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    char buf[512] = {};
+    int len = 0;
+    void mark(const char *name)
+    {
+      if (!on) return;
+      auto now = std::chrono::steady_clock::now();
+      double ms = std::chrono::duration<double, std::milli>(now - t).count();
+      t = now;
+      if (len < (int)sizeof buf - 64) len += snprintf(buf + len, sizeof buf - len, " %s %.2f", name, ms);
+    }
+    void print(int64_t vol) const
+    {
+      if (on) fprintf(stderr, "vgpu create (%lld cells, ms):%s\n", (long long)vol, buf);
+    }
+  };
+
   int create(const vgpu_problem *in)
+  {
+    PhaseClock pc;
+    int rc = create_phases(in, pc);
+    pc.print(vol);
+    return rc;
+  }
+
+  int create_phases(const vgpu_problem *in, PhaseClock &pc)
   {
     p = *in;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -325,6 +365,7 @@ struct Engine : EngineBase {
     if (mem.alloc(&fields, (size_t)vol * 6)) return VGPU_ENOMEM;
     CK(cudaMemset(fields, 0, sizeof(T) * vol * 6));
     for (int c = 0; c < 6; c++) g.F[c] = fields + (int64_t)c * vol;
+    pc.mark("fields");
     // Coefficients: a one-byte index and a table where the mesh allows it
     // (at most 256 distinct tuples), else the full volumes.
     if (int rc = setup_coef_index()) return rc;
@@ -351,6 +392,7 @@ struct Engine : EngineBase {
     }
     if (mem.alloc(&d_step, 1)) return VGPU_ENOMEM;
     CK(cudaMemset(d_step, 0, sizeof(uint64_t)));
+    pc.mark("coef");
 
     // Bulk limits.
     for (int c = 0; c < 3; c++) {
@@ -365,14 +407,20 @@ struct Engine : EngineBase {
     if (int rc = setup_debye()) return rc;
     if (int rc = setup_sibc()) return rc;
     if (int rc = setup_sources()) return rc;
+    pc.mark("pml-mur-debye-sibc-src");
     if (int rc = setup_planewaves()) return rc;
+    pc.mark("tfsf");
     setup_ghost();
     if (int rc = setup_observers()) return rc;
+    pc.mark("observers");
     if (int rc = setup_sweeps()) return rc;
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
+    pc.mark("sweeps");
     stats.device_bytes = mem.bytes;
-    return capture_graph();
+    int rc = capture_graph();
+    pc.mark("graph");
+    return rc;
   }
 
   static Box unite(const Box b[3])
@@ -1392,7 +1440,7 @@ struct Engine : EngineBase {
   {
     cudaGraph_t gr;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    enqueue_steps(kChunk);
+    enqueue_steps(kGraphSteps);
     CK(cudaStreamEndCapture(s, &gr));
     cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
     cudaGraphDestroy(gr);
@@ -1432,11 +1480,11 @@ struct Engine : EngineBase {
     if (p.num_bin > 0)
       if (int rc = bin_deliver(q)) return rc;
     if (m == (uint64_t)kChunk) {
-      CK(cudaGraphLaunch(graph, s));
+      for (int r = 0; r < kChunk / kGraphSteps; r++) CK(cudaGraphLaunch(graph, s));
     } else {
       if (int rc = enqueue_steps((int)m)) return rc;
     }
-    stats.kernel_launches += m * launches_per_step + 1;
+    stats.kernel_launches += m * launches_per_step + (m == (uint64_t)kChunk ? kChunk / kGraphSteps : 1);
     step += m;
     // Output rows produced in this block.
     const uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
@@ -1613,7 +1661,17 @@ struct Engine : EngineBase {
 
 struct vgpu_engine {
   EngineBase *impl;
+  int dev;   // the CUDA device the engine was created on
 };
+
+// The engine's implementation, with its device made current on the calling
+// thread: engines may be driven from threads other than the creating one.
+static EngineBase *on_dev(const vgpu_engine *e)
+{
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != e->dev) cudaSetDevice(e->dev);
+  return e->impl;
+}
 
 static int validate(const vgpu_problem *p)
 {
@@ -1688,44 +1746,61 @@ extern "C" int vgpu_create(const vgpu_problem *p, vgpu_engine **out)
     delete impl;
     return rc;
   }
-  *out = new vgpu_engine{ impl };
+  *out = new vgpu_engine{ impl, dev };
+  return 0;
+}
+
+extern "C" int vgpu_set_device(int32_t device)
+{
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return set_err(VGPU_ENODEV, "cudaSetDevice(%d): %s", (int)device, cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int vgpu_get_device(int32_t *device)
+{
+  if (!device) return set_err(VGPU_EINVAL, "null argument");
+  int d = 0;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) return set_err(VGPU_ENODEV, "cudaGetDevice: %s", cudaGetErrorString(e));
+  *device = d;
   return 0;
 }
 
 extern "C" int vgpu_run(vgpu_engine *e, uint64_t nsteps)
 {
   if (!e) return set_err(VGPU_EINVAL, "null engine");
-  return e->impl->run(nsteps);
+  return on_dev(e)->run(nsteps);
 }
 
 extern "C" int vgpu_read_td(vgpu_engine *e, double *out, uint64_t steps)
 {
   if (!e || !out) return set_err(VGPU_EINVAL, "null argument");
-  return e->impl->read_td(out, steps);
+  return on_dev(e)->read_td(out, steps);
 }
 
 extern "C" int vgpu_read_dft(vgpu_engine *e, double *re, double *im)
 {
   if (!e || !re || !im) return set_err(VGPU_EINVAL, "null argument");
-  return e->impl->read_dft(re, im);
+  return on_dev(e)->read_dft(re, im);
 }
 
 extern "C" int vgpu_read_field(vgpu_engine *e, int32_t c, double *out)
 {
   if (!e || !out || c < 0 || c > 5) return set_err(VGPU_EINVAL, "invalid argument");
-  return e->impl->read_field(c, out);
+  return on_dev(e)->read_field(c, out);
 }
 
 extern "C" int vgpu_write_field(vgpu_engine *e, int32_t c, const double *in)
 {
   if (!e || !in || c < 0 || c > 5) return set_err(VGPU_EINVAL, "invalid argument");
-  return e->impl->write_field(c, in);
+  return on_dev(e)->write_field(c, in);
 }
 
 extern "C" int vgpu_check_finite(vgpu_engine *e)
 {
   if (!e) return set_err(VGPU_EINVAL, "null engine");
-  return e->impl->check_finite();
+  return on_dev(e)->check_finite();
 }
 
 extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl->step : 0; }
@@ -1733,19 +1808,19 @@ extern "C" uint64_t vgpu_current_step(const vgpu_engine *e) { return e ? e->impl
 extern "C" int vgpu_enqueue(vgpu_engine *e, uint64_t max_steps, uint64_t *queued)
 {
   if (!e || !queued) return set_err(VGPU_EINVAL, "null argument");
-  return e->impl->enqueue(max_steps, queued);
+  return on_dev(e)->enqueue(max_steps, queued);
 }
 
 extern "C" int vgpu_query(vgpu_engine *e)
 {
   if (!e) return set_err(VGPU_EINVAL, "null engine");
-  return e->impl->query();
+  return on_dev(e)->query();
 }
 
 extern "C" int vgpu_synchronize(vgpu_engine *e)
 {
   if (!e) return set_err(VGPU_EINVAL, "null engine");
-  return e->impl->synchronize();
+  return on_dev(e)->synchronize();
 }
 
 extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint64_t *steps)
@@ -1753,7 +1828,7 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
   if (n < 0 || (n && (!engines || !steps))) return set_err(VGPU_EINVAL, "invalid batch");
   for (int32_t i = 0; i < n; i++) {
     if (!engines[i]) return set_err(VGPU_EINVAL, "null engine %d in batch", (int)i);
-    if (int rc = engines[i]->impl->check_steps(steps[i])) return rc;
+    if (int rc = on_dev(engines[i])->check_steps(steps[i])) return rc;
   }
   std::vector<uint64_t> left(steps, steps + n);
   for (bool any = true; any;) {
@@ -1761,7 +1836,7 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
     for (int32_t i = 0; i < n; i++) {
       if (!left[i]) continue;
       uint64_t m = 0;
-      if (int rc = engines[i]->impl->enqueue(left[i], &m)) return rc;
+      if (int rc = on_dev(engines[i])->enqueue(left[i], &m)) return rc;
       // An engine listed twice can reach its last step before its count.
       if (!m) return set_err(VGPU_EINVAL, "engine %d in batch reached its last step", (int)i);
       left[i] -= m;
@@ -1770,7 +1845,7 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
   }
   int rc = 0;
   for (int32_t i = 0; i < n; i++) {
-    int r = engines[i]->impl->synchronize();
+    int r = on_dev(engines[i])->synchronize();
     if (r && !rc) rc = r;
   }
   return rc;
@@ -1779,14 +1854,14 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
 extern "C" int vgpu_sweep_points(const vgpu_engine *e, int32_t kernel, uint64_t *bulk_points, uint64_t *pml_points)
 {
   if (!e || !bulk_points || !pml_points) return set_err(VGPU_EINVAL, "null argument");
-  return e->impl->sweep_points(kernel, bulk_points, pml_points);
+  return on_dev(e)->sweep_points(kernel, bulk_points, pml_points);
 }
 
 extern "C" int vgpu_set_bin_sink(vgpu_engine *e, vgpu_bin_sink sink, void *user)
 {
   if (!e) return set_err(VGPU_EINVAL, "null engine");
-  e->impl->bin_sink = sink;
-  e->impl->bin_user = user;
+  on_dev(e)->bin_sink = sink;
+  on_dev(e)->bin_user = user;
   return 0;
 }
 
@@ -1794,13 +1869,13 @@ extern "C" int vgpu_time_kernel(vgpu_engine *e, int32_t kernel, int32_t warmup, 
                                 uint64_t *points)
 {
   if (!e || !ms || !points || iters < 0 || warmup < 0) return set_err(VGPU_EINVAL, "invalid argument");
-  return e->impl->time_kernel(kernel, warmup, iters, ms, points);
+  return on_dev(e)->time_kernel(kernel, warmup, iters, ms, points);
 }
 
 extern "C" int vgpu_get_stats(const vgpu_engine *e, vgpu_stats *st)
 {
   if (!e || !st) return set_err(VGPU_EINVAL, "null argument");
-  *st = e->impl->stats;
+  *st = on_dev(e)->stats;
   return 0;
 }
 
@@ -1856,6 +1931,6 @@ extern "C" int vgpu_dft_accumulate_static(const double *samples, int32_t num_ser
 extern "C" void vgpu_destroy(vgpu_engine *e)
 {
   if (!e) return;
-  delete e->impl;
+  delete on_dev(e);
   delete e;
 }

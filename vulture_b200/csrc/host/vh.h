@@ -253,6 +253,12 @@ typedef struct vhost vh_ctx;
 int vh_fail(vh_ctx *c, const char *fmt, ...);
 void vh_log(vh_ctx *c, int verbose_only, const char *fmt, ...);
 
+/* Runs fn(ctx, lo, hi) over [begin, end) split into contiguous ranges on
+ * up to 16 threads; one call on the calling thread when work (the points
+ * the whole range touches) is small.  The ranges must touch disjoint
+ * memory. */
+void vh_parallel_for(int begin, int end, int64_t work, void (*fn)(void *ctx, int lo, int hi), void *ctx);
+
 /* Indexing helpers. */
 static inline int64_t vh_idx(const vh_ctx *c, int i, int j, int k)
 {

@@ -8,10 +8,55 @@
  */
 #include <assert.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
+#include <unistd.h>
 
 #include "vh.h"
+
+typedef struct {
+  void (*fn)(void *, int, int);
+  void *ctx;
+  int lo, hi;
+} vh_range_job;
+
+static void *range_main(void *arg)
+{
+  vh_range_job *j = arg;
+  j->fn(j->ctx, j->lo, j->hi);
+  return NULL;
+}
+
+void vh_parallel_for(int begin, int end, int64_t work, void (*fn)(void *ctx, int lo, int hi), void *ctx)
+{
+  const int n = end - begin;
+  long cores = sysconf(_SC_NPROCESSORS_ONLN);
+  int nt = cores > 16 ? 16 : (cores < 1 ? 1 : (int)cores);
+  if (work < (1 << 18) || n < 2) nt = 1;
+  if (nt > n) nt = n;
+  if (nt <= 1) {
+    if (n > 0) fn(ctx, begin, end);
+    return;
+  }
+  pthread_t th[16];
+  vh_range_job jobs[16];
+  int started[16] = { 0 };
+  for (int t = 0; t < nt; t++) {
+    jobs[t] = (vh_range_job){ fn, ctx, begin + (int)((int64_t)n * t / nt), begin + (int)((int64_t)n * (t + 1) / nt) };
+    /* The first range runs here; a thread that fails to start runs its
+     * range here as well. */
+    if (t > 0) started[t] = pthread_create(&th[t], NULL, range_main, &jobs[t]) == 0;
+  }
+  range_main(&jobs[0]);
+  for (int t = 1; t < nt; t++) {
+    if (started[t]) pthread_join(th[t], NULL);
+    else range_main(&jobs[t]);
+  }
+}
+
+static double *alloc_volume(size_t n);
 
 int vh_outer_type(const vh_ctx *c, int face) { return c->bnds[c->ext_bnd[face]].type; }
 
@@ -153,7 +198,7 @@ int vh_init_grid(vh_ctx *c)
   init_field_array_limits(c);
   int64_t vol = (int64_t)c->n[0] * c->n[1] * c->n[2];
   for (int q = 0; q < 9; q++) {
-    c->coef[q] = calloc((size_t)vol, sizeof(double));
+    c->coef[q] = alloc_volume((size_t)vol);
     if (!c->coef[q]) return vh_fail(c, "Failed to allocate grid coefficient arrays (%lld cells)", (long long)vol);
   }
   init_cell_edges(c);
@@ -244,6 +289,53 @@ int vh_init_media(vh_ctx *c)
   return 0;
 }
 
+typedef struct {
+  vh_ctx *c;
+  const vh_medium *m;
+  int flim[6][6];
+} paint_job;
+
+/* Planes lo..hi-1 of every component's limits. */
+static void paint_range(void *ctx, int lo, int hi)
+{
+  paint_job *p = ctx;
+  vh_ctx *c = p->c;
+  const vh_medium *m = p->m;
+  for (int f = EX; f <= HZ; f++) {
+    double *a = f <= EZ ? c->coef[f] : NULL;
+    double *b = f <= EZ ? c->coef[3 + f] : c->coef[6 + f - HX];
+    const int ia = p->flim[f][XLO] > lo ? p->flim[f][XLO] : lo;
+    const int ib = p->flim[f][XHI] < hi - 1 ? p->flim[f][XHI] : hi - 1;
+    for (int i = ia; i <= ib; i++)
+      for (int j = p->flim[f][YLO]; j <= p->flim[f][YHI]; j++)
+        for (int k = p->flim[f][ZLO]; k <= p->flim[f][ZHI]; k++) {
+          int64_t q = vh_idx(c, i, j, k);
+          if (a) { a[q] = m->alpha; b[q] = m->beta; }
+          else b[q] = m->gamma;
+        }
+  }
+}
+
+static void zero_range(void *ctx, int lo, int hi)
+{
+  memset((char *)ctx + ((size_t)lo << 21), 0, (size_t)(hi - lo) << 21);
+}
+
+/* A zeroed volume of n doubles: 2 MiB aligned and advised for huge pages,
+ * zeroed by several threads, so first touch costs few page faults. */
+static double *alloc_volume(size_t n)
+{
+  const size_t huge = (size_t)1 << 21;
+  const size_t bytes = (n * sizeof(double) + huge - 1) / huge * huge;
+  void *p = NULL;
+  if (posix_memalign(&p, huge, bytes ? bytes : huge)) return NULL;
+#ifdef MADV_HUGEPAGE
+  madvise(p, bytes, MADV_HUGEPAGE);
+#endif
+  vh_parallel_for(0, (int)(bytes / huge), (int64_t)(bytes / sizeof(double)), zero_range, p);
+  return p;
+}
+
 /* Paint a medium's coefficients over a box (src/grid.c:1726-1873). */
 void vh_set_medium_on_grid(vh_ctx *c, const int gbbox[6], int medium, unsigned char mask)
 {
@@ -252,18 +344,18 @@ void vh_set_medium_on_grid(vh_ctx *c, const int gbbox[6], int medium, unsigned c
   vh_mask_to_bool(incl, mask);
   if (vh_bbox_type(gbbox) == BB_POINT) return;
   vh_set_field_limits(gbbox, flim, incl);
-  const vh_medium *m = &c->media[medium];
-  for (int f = EX; f <= HZ; f++) {
-    double *a = f <= EZ ? c->coef[f] : NULL;
-    double *b = f <= EZ ? c->coef[3 + f] : c->coef[6 + f - HX];
-    for (int i = flim[f][XLO]; i <= flim[f][XHI]; i++)
-      for (int j = flim[f][YLO]; j <= flim[f][YHI]; j++)
-        for (int k = flim[f][ZLO]; k <= flim[f][ZHI]; k++) {
-          int64_t q = vh_idx(c, i, j, k);
-          if (a) { a[q] = m->alpha; b[q] = m->beta; }
-          else b[q] = m->gamma;
-        }
+  paint_job job = { c, &c->media[medium], { 0 } };
+  memcpy(job.flim, flim, sizeof flim);
+  int64_t work = 0;
+  for (int f = EX; f <= HZ; f++)
+    work += (int64_t)(flim[f][XHI] - flim[f][XLO] + 1) * (flim[f][YHI] - flim[f][YLO] + 1) *
+            (flim[f][ZHI] - flim[f][ZLO] + 1);
+  int i0 = flim[EX][XLO], i1 = flim[EX][XHI];
+  for (int f = EY; f <= HZ; f++) {
+    if (flim[f][XLO] < i0) i0 = flim[f][XLO];
+    if (flim[f][XHI] > i1) i1 = flim[f][XHI];
   }
+  vh_parallel_for(i0, i1 + 1, work, paint_range, &job);
 }
 
 /* src/grid.c:1146-1162 */
@@ -465,6 +557,47 @@ static void set_pml_parameters(vh_ctx *c)
   }
 }
 
+typedef struct {
+  vh_ctx *c;
+  int r;
+  int lim[6][6];
+} pml_copy_job;
+
+/* Region r's copies for split-axis coordinates lo..hi-1 (axis j for the X
+ * regions, i for the others). */
+static void pml_copy_range(void *ctx, int lo, int hi)
+{
+  pml_copy_job *p = ctx;
+  vh_ctx *c = p->c;
+  const int r = p->r, a = r / 2, off = (r % 2 == 0) ? +1 : -1, d = a == 0 ? 1 : 0;
+  const int plane = c->gibox[r];
+  for (int f = EX; f <= HZ; f++) {
+    /* Components normal to the region's axis (E) or tangential (H) read one
+     * layer inside the inner box; the others read on the boundary plane. */
+    int src_off;
+    if (f <= EZ) src_off = (f == a) ? off : 0;
+    else src_off = (f - HX == a) ? 0 : off;
+    const int src = plane + src_off;
+    int l[6];
+    memcpy(l, p->lim[f], sizeof l);
+    if (l[2 * d] < lo) l[2 * d] = lo;
+    if (l[2 * d + 1] > hi - 1) l[2 * d + 1] = hi - 1;
+    for (int i = l[XLO]; i <= l[XHI]; i++)
+      for (int j = l[YLO]; j <= l[YHI]; j++)
+        for (int k = l[ZLO]; k <= l[ZHI]; k++) {
+          int s[3] = { i, j, k };
+          s[a] = src;
+          int64_t qd = vh_idx(c, i, j, k), qs = vh_idx(c, s[0], s[1], s[2]);
+          if (f <= EZ) {
+            c->coef[f][qd] = c->coef[f][qs];
+            c->coef[3 + f][qd] = c->coef[3 + f][qs];
+          } else {
+            c->coef[6 + f - HX][qd] = c->coef[6 + f - HX][qs];
+          }
+        }
+  }
+}
+
 /* Carry inner-boundary media into the PML, Z then Y then X (src/pml.c:445-629). */
 static void init_pml_material_arrays(vh_ctx *c)
 {
@@ -474,29 +607,21 @@ static void init_pml_material_arrays(vh_ctx *c)
   for (int r = 0; r < 6; r++) vh_set_field_limits(c->pbox[r], lim[r], incl[r]);
   static const int order[6] = { ZLO, ZHI, YLO, YHI, XLO, XHI };
   for (int o = 0; o < 6; o++) {
-    int r = order[o], a = r / 2, off = (r % 2 == 0) ? +1 : -1;
-    int plane = c->gibox[r];
+    const int r = order[o];
+    pml_copy_job job = { c, r, { { 0 } } };
+    memcpy(job.lim, lim[r], sizeof job.lim);
+    /* Split along an axis other than the copy axis, so no range reads a
+     * plane another range writes. */
+    const int d = r / 2 == 0 ? 1 : 0;
+    int lo = 1 << 30, hi = -(1 << 30);
+    int64_t work = 0;
     for (int f = EX; f <= HZ; f++) {
-      /* Components normal to the region's axis (E) or tangential (H) read one
-       * layer inside the inner box; the others read on the boundary plane. */
-      int src_off;
-      if (f <= EZ) src_off = (f == a) ? off : 0;
-      else src_off = (f - HX == a) ? 0 : off;
-      int src = plane + src_off;
-      for (int i = lim[r][f][XLO]; i <= lim[r][f][XHI]; i++)
-        for (int j = lim[r][f][YLO]; j <= lim[r][f][YHI]; j++)
-          for (int k = lim[r][f][ZLO]; k <= lim[r][f][ZHI]; k++) {
-            int s[3] = { i, j, k };
-            s[a] = src;
-            int64_t qd = vh_idx(c, i, j, k), qs = vh_idx(c, s[0], s[1], s[2]);
-            if (f <= EZ) {
-              c->coef[f][qd] = c->coef[f][qs];
-              c->coef[3 + f][qd] = c->coef[3 + f][qs];
-            } else {
-              c->coef[6 + f - HX][qd] = c->coef[6 + f - HX][qs];
-            }
-          }
+      if (lim[r][f][2 * d] < lo) lo = lim[r][f][2 * d];
+      if (lim[r][f][2 * d + 1] > hi) hi = lim[r][f][2 * d + 1];
+      work += (int64_t)(lim[r][f][XHI] - lim[r][f][XLO] + 1) * (lim[r][f][YHI] - lim[r][f][YLO] + 1) *
+              (lim[r][f][ZHI] - lim[r][f][ZLO] + 1);
     }
+    vh_parallel_for(lo, hi + 1, work, pml_copy_range, &job);
   }
 }
 

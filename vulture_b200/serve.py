@@ -1,26 +1,32 @@
 """Serving loop over the asynchronous engine entry points.
 
 Solve requests (a mesh text, an arrival time and a precision) are admitted
-while their estimated device footprint fits an HBM budget, and the admitted
-solves share the device by continuous batching: every turn each active solve
-whose stream has drained gets its next 64-step blocks queued
-(vgpu_enqueue), a finished solve is retired at once (its observers read, its
-memory freed) and the next waiting request takes its place.  Each solve runs
-on its own engine and stream, so its results are the ones a solo run gives.
+first come, first served while a solve slot is free and their estimated
+device footprint fits an HBM budget.  The admitted solves share the device
+by continuous batching: every turn each active solve whose stream has
+drained gets its next 64-step blocks queued (vgpu_enqueue), a finished solve
+is retired at once (its observers read, its memory freed) and the next
+waiting request takes its place.  Mesh set-up and engine creation run on
+worker threads, so the device keeps stepping the active solves meanwhile.
+Each solve runs on its own engine and stream, so its results are the ones a
+solo run gives.
 
 The reference runs one mesh per process (src/vulture.c:77-197); serving has
 no counterpart there and is built on the same per-mesh engine.
 """
 from __future__ import annotations
 
+import ctypes as C
 import os
 import tempfile
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
 
+from . import _native as N
 from .solver import GpuRun, Mesh
 
 _WORD = {"fp32": 4, "fp64": 8}
@@ -33,6 +39,7 @@ class Request:
     precision: str = "fp32"
     tag: str = ""
     admitted: float | None = None
+    started: float | None = None  # engine created, first block queued
     completed: float | None = None
     cell_updates: int = 0
     td: np.ndarray | None = None
@@ -58,12 +65,23 @@ def footprint_estimate(mesh: Mesh, precision: str) -> int:
 
 
 class Server:
-    """Admission by HBM budget plus continuous batching of 64-step blocks."""
+    """Admission by solve slots and HBM budget, continuous batching of
+    64-step blocks.
 
-    def __init__(self, budget_bytes: int, max_inflight_blocks: int = 2, block_steps: int = 64):
+    budget_bytes: device bytes the admitted solves may hold together (by
+    their estimates); a request larger than the whole budget runs alone.
+    max_active: solves stepping side by side.  max_inflight_blocks: blocks
+    queued per solve each time its stream drains.  workers: host threads
+    that parse meshes and create engines.
+    """
+
+    def __init__(self, budget_bytes: int, max_active: int = 4, max_inflight_blocks: int = 2,
+                 block_steps: int = 64, workers: int = 2):
         self.budget = int(budget_bytes)
+        self.max_active = max(1, int(max_active))
         self.max_inflight = max(1, int(max_inflight_blocks))
         self.block_steps = block_steps
+        self.workers = max(1, int(workers))
         self.peak_bytes = 0
         self.peak_active = 0
 
@@ -71,41 +89,58 @@ class Server:
         """Serve the requests (sorted by arrival); returns them completed."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending = deque(reqs)
-        waiting: deque = deque()
-        active = []                     # (request, mesh, run, path)
+        waiting: deque = deque()      # arrived, not admitted: [request, parse future]
+        creating = []                 # admitted: (request, mesh, path, create future)
+        active = []                   # stepping: (request, mesh, run, path)
         used = 0
-        head = None                     # the parsed mesh of the next request to admit
         tmp = tempfile.mkdtemp(prefix="vgpu_serve_")
+        dev = C.c_int32()
+        N.check_gpu(N.lib().vgpu_get_device(C.byref(dev)))
+        # Worker threads create engines on the calling thread's device.
+        pool = ThreadPoolExecutor(self.workers, initializer=lambda: N.check_gpu(N.lib().vgpu_set_device(dev.value)))
+
+        def parse(r):
+            path = os.path.join(tmp, f"req{id(r)}.msh")
+            with open(path, "w") as f:
+                f.write(r.mesh_text)
+            mesh = Mesh(path)
+            return mesh, path, footprint_estimate(mesh, r.precision)
+
         t0 = time.perf_counter()
         try:
-            while pending or waiting or active:
+            while pending or waiting or creating or active:
                 now = time.perf_counter() - t0
                 while pending and pending[0].arrival <= now:
-                    waiting.append(pending.popleft())
-                # Admission: first come, first served, while the estimate fits
-                # (a request larger than the whole budget runs alone).
-                while waiting:
-                    r = waiting[0]
-                    if head is None or head[0] is not r:
-                        path = os.path.join(tmp, f"req{id(r)}.msh")
-                        with open(path, "w") as f:
-                            f.write(r.mesh_text)
-                        mesh = Mesh(path)
-                        head = (r, mesh, path, footprint_estimate(mesh, r.precision))
-                    _, mesh, path, est = head
-                    if active and used + est > self.budget:
+                    waiting.append([pending.popleft(), None])
+                # Parse the first few waiting meshes ahead of admission.
+                for w in list(waiting)[: self.workers]:
+                    if w[1] is None:
+                        w[1] = pool.submit(parse, w[0])
+                # Admission, first come first served.
+                while waiting and waiting[0][1].done() and len(active) + len(creating) < self.max_active:
+                    r, fut = waiting[0]
+                    mesh, path, est = fut.result()
+                    if (active or creating) and used + est > self.budget:
                         break
                     waiting.popleft()
-                    head = None
                     r.estimate = est
                     r.admitted = time.perf_counter() - t0
-                    run = GpuRun(mesh, r.precision)
-                    r.device_bytes = int(run.stats().device_bytes)
                     used += est
-                    active.append((r, mesh, run, path))
+                    creating.append((r, mesh, path, pool.submit(GpuRun, mesh, r.precision)))
                 self.peak_bytes = max(self.peak_bytes, used)
-                self.peak_active = max(self.peak_active, len(active))
                 progressed = False
+                still_creating = []
+                for r, mesh, path, fut in creating:
+                    if fut.done():
+                        run = fut.result()
+                        r.device_bytes = int(run.stats().device_bytes)
+                        r.started = time.perf_counter() - t0
+                        active.append((r, mesh, run, path))
+                        progressed = True
+                    else:
+                        still_creating.append((r, mesh, path, fut))
+                creating = still_creating
+                self.peak_active = max(self.peak_active, len(active))
                 still = []
                 for r, mesh, run, path in active:
                     if not run.done():
@@ -131,16 +166,22 @@ class Server:
                     still.append((r, mesh, run, path))
                 active = still
                 if not progressed:
-                    if not active and pending:
+                    if not active and not creating and not waiting and pending:
                         time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.01)))
                     else:
                         time.sleep(50e-6)
         finally:
+            pool.shutdown(wait=True)
             for r, mesh, run, path in active:
                 run.close()
                 mesh.close()
-            if head is not None:
-                head[1].close()
+            for r, mesh, path, fut in creating:
+                if fut.exception() is None:
+                    fut.result().close()
+                mesh.close()
+            for r, fut in waiting:
+                if fut is not None and fut.exception() is None:
+                    fut.result()[0].close()
             try:
                 for f in os.listdir(tmp):
                     os.unlink(os.path.join(tmp, f))
@@ -150,10 +191,57 @@ class Server:
         return reqs
 
 
+def solve_batch(meshes, precision: str = "fp32", workers: int = 3, max_inflight_blocks: int = 2,
+                block_steps: int = 64):
+    """Solve independent meshes to their last step on the current device.
+
+    Engines are created on worker threads; each one starts stepping as soon
+    as it exists, and every engine whose stream has drained gets its next
+    blocks queued, so creation overlaps the stepping of the engines before
+    it.  Returns the finished GpuRun objects in the meshes' order, their
+    results ready to read."""
+    dev = C.c_int32()
+    N.check_gpu(N.lib().vgpu_get_device(C.byref(dev)))
+    pool = ThreadPoolExecutor(max(1, workers), initializer=lambda: N.check_gpu(N.lib().vgpu_set_device(dev.value)))
+    futs = [pool.submit(GpuRun, m, precision) for m in meshes]
+    runs = [None] * len(meshes)
+    left = set(range(len(meshes)))
+    try:
+        while left:
+            progressed = False
+            for q in list(left):
+                r = runs[q]
+                if r is None:
+                    if not futs[q].done():
+                        continue
+                    r = runs[q] = futs[q].result()
+                if not r.done():
+                    continue
+                progressed = True
+                if r.step >= r.mesh.num_steps:
+                    r.synchronize()
+                    left.discard(q)
+                    continue
+                for _ in range(max_inflight_blocks):
+                    if not r.enqueue(block_steps):
+                        break
+            if not progressed:
+                time.sleep(50e-6)
+    except BaseException:
+        pool.shutdown(wait=True)
+        for q, f in enumerate(futs):
+            if f.done() and f.exception() is None:
+                f.result().close()
+        raise
+    pool.shutdown(wait=True)
+    return runs
+
+
 def latency_summary(reqs):
-    """p50 / p99 latency (arrival to completion) and completed solves/s."""
+    """p50 / p99 latency (arrival to completion), mean, completed solves/s."""
     lat = np.array([r.latency for r in reqs])
     span = max(r.completed for r in reqs) - min(r.arrival for r in reqs)
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()),
             "solves_per_s": len(reqs) / span if span > 0 else float("inf"),
             "cell_updates": int(sum(r.cell_updates for r in reqs))}
