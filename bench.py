@@ -335,6 +335,10 @@ def run_gpu_arm(args):
             "config": {"workload": "graded 200x160x120, UPML8, Debye, TFSF, 64x64x200 DFT plane + 16 TD",
                        "n_out_cells": n_out, "replicas": world, "l2": "inputs larger than L2 (~370 MB/GPU)",
                        "precision": prec},
+            "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec],
+                              "achieved_gbs": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9,
+                              "frac": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9 / peak,
+                              "what": "whole step: cell-updates/s x 27 algorithmic words per cell, of measured"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": tr, "kernels": kern,
@@ -446,6 +450,9 @@ def run_batch_workload(args):
                                 "beforehand"},
             "mcell_updates_per_s": cell_updates / step_s / 1e6,
             "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
+            "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG["fp32"],
+                              "frac": cell_updates / step_s * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9 / peak,
+                              "what": "stepping: cell-updates/s x 27 algorithmic words per cell, of measured"},
             "run_batch": {"create_s": create_s, "step_s": step_s},
             "fp64_sequential_solves_per_s": sps64, "speedup_vs_fp64_sequential": sps32 / sps64,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
