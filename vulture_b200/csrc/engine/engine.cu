@@ -324,7 +324,7 @@ struct Engine : EngineBase {
   struct PhaseClock {
     bool on = getenv("VGPU_TRACE") != nullptr;
     std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
-    char buf[512] = {};
+    char buf[1024] = {};
     int len = 0;
     void mark(const char *name)
     {
@@ -344,12 +344,20 @@ struct Engine : EngineBase {
   {
     PhaseClock pc;
     int rc = create_phases(in, pc);
+    pclock = nullptr;
     pc.print(vol);
     return rc;
   }
 
+  PhaseClock *pclock = nullptr;   // set while create() runs
+  void mark(const char *name)
+  {
+    if (pclock) pclock->mark(name);
+  }
+
   int create_phases(const vgpu_problem *in, PhaseClock &pc)
   {
+    pclock = &pc;
     p = *in;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
@@ -741,15 +749,12 @@ struct Engine : EngineBase {
     std::vector<Part> parts(tv.n);
     auto make = [&](int q, int i, int j, int k, std::vector<TfsfEntry<T>> &ent, std::vector<int> &pos) {
       const TfsfItem &it = tv.it[q];
+      // Line length and coefficients are filled in on the device
+      // (k_tfsf_prepare), from the arrays the sweeps read.
       TfsfEntry<T> d;
       memset(&d, 0, sizeof d);
-      const int64_t hq = ((int64_t)i * p.n[1] + j) * p.n[2] + k;
-      const int gi = it.axis == 0 ? i : it.axis == 1 ? j : k;
       d.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
       d.meta = q;
-      d.idv = (T)(efield ? p.idh[it.axis][gi] : p.ide[it.axis][gi]);
-      d.ca = efield ? (T)p.coef[it.c][hq] : (T)0;
-      d.cb = efield ? (T)p.coef[3 + it.c][hq] : (T)p.coef[6 + it.c - HX][hq];
       ent.push_back(d);
       int sp[3] = { i, j, k };
       sp[it.axis] += it.shift;
@@ -784,12 +789,14 @@ struct Engine : EngineBase {
               if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.multi, pt.mpos);
           }
     };
+    mark(efield ? "tfsf-e-start" : "tfsf-h-start");
     {
       std::vector<std::thread> pool;
       for (int q = 1; q < tv.n; q++) pool.emplace_back(enumerate, q);
       if (tv.n > 0) enumerate(0);
       for (auto &t : pool) t.join();
     }
+    mark("enumerate");
     // Points of one entry first, then the multi-entry points' runs.
     size_t ns = 0, nm = 0;
     for (const Part &pt : parts) {
@@ -812,6 +819,7 @@ struct Engine : EngineBase {
       pos.insert(pos.end(), pt.mpos.begin(), pt.mpos.end());
     }
     mstart.push_back((int)ne);
+    mark("merge");
     tl.nentries = (int64_t)ne;
     tl.nsingle = (int)ns;
     tl.nmulti = (int)mstart.size() - 1;
@@ -823,9 +831,11 @@ struct Engine : EngineBase {
     tl.ent = de;
     tl.pos = dpos;
     tl.mstart = dm;
-    k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, s>>>(L.pv, tv, tl);
+    mark("upload");
+    k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, s>>>(g, L.pv, tv, tl, efield ? 1 : 0);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    mark("prepare");
     return 0;
   }
 
@@ -854,20 +864,30 @@ struct Engine : EngineBase {
       Part &pt = parts[w];
       std::map<Key, int> seen;
       int last = -1;
-      Key lastk{};
+      uint64_t lastraw[6] = {};   // bit patterns of the previous cell's doubles
+      const double *src[6];
+      for (int c = 0; c < count; c++) src[c] = p.coef[first + c];
       for (int i = i0; i < i1 && !pt.overflow; i++)
         for (int j = 0; j < p.n[1]; j++) {
           const int64_t hrow = ((int64_t)i * p.n[1] + j) * p.n[2];
           uint8_t *irow = idx.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
           for (int k = 0; k < p.n[2]; k++) {
-            Key key{};
-            for (int c = 0; c < count; c++) key.v[c] = (T)p.coef[first + c][hrow + k];
-            int q = -1;
-            if (last >= 0 && memcmp(key.v, lastk.v, sizeof key.v) == 0) q = last;
-            if (q < 0) {
-              auto it = seen.find(key);
-              if (it != seen.end()) q = it->second;
+            // Same doubles as the previous cell (the common case): same tuple.
+            uint64_t raw[6];
+            bool same = last >= 0;
+            for (int c = 0; c < count; c++) {
+              memcpy(&raw[c], src[c] + hrow + k, sizeof(double));
+              same = same && raw[c] == lastraw[c];
             }
+            if (same) {
+              irow[k] = (uint8_t)last;
+              continue;
+            }
+            Key key{};
+            for (int c = 0; c < count; c++) key.v[c] = (T)src[c][hrow + k];
+            int q = -1;
+            auto it = seen.find(key);
+            if (it != seen.end()) q = it->second;
             if (q < 0) {
               if (seen.size() == 256) {
                 pt.overflow = true;
@@ -878,7 +898,7 @@ struct Engine : EngineBase {
               pt.keys.push_back(key);
             }
             last = q;
-            lastk = key;
+            memcpy(lastraw, raw, sizeof raw);
             irow[k] = (uint8_t)q;
           }
         }
@@ -1195,6 +1215,7 @@ struct Engine : EngineBase {
       (es ? maps_e : maps_h).wn = wn > kSweepKW ? 0 : wn;
       SweepLaunch *L = es ? sw_e : sw_h;
       const bool comp = (es ? cie : cih).idx != nullptr;
+      mark("tiles");
       if (es) {
         if (int rc = prepare_launch<true, false>(L[0], bulk, comp)) return rc;
         if (int rc = prepare_launch<true, true>(L[1], pml, comp)) return rc;
@@ -1202,6 +1223,7 @@ struct Engine : EngineBase {
         if (int rc = prepare_launch<false, false>(L[0], bulk, comp)) return rc;
         if (int rc = prepare_launch<false, true>(L[1], pml, comp)) return rc;
       }
+      mark("headers");
     }
     if (int rc = make_sweep_maps(maps_e, true)) return rc;
     if (int rc = make_sweep_maps(maps_h, false)) return rc;
@@ -1238,7 +1260,10 @@ struct Engine : EngineBase {
   int setup_coef_index()
   {
     if (int rc = build_index(0, 6, cie)) return rc;
-    return build_index(6, 3, cih);
+    mark("index-e");
+    int rc = build_index(6, 3, cih);
+    mark("index-h");
+    return rc;
   }
 
   void setup_ghost()
@@ -1357,6 +1382,11 @@ struct Engine : EngineBase {
 
   // One time step, in the order of src/simulation.c:156-222, `rel` steps
   // past the device step counter.
+  static int64_t tfsf_threads(const TfsfList<T> &l)
+  {
+    return (l.nsingle + kTfsfPerThread - 1) / kTfsfPerThread + l.nmulti;
+  }
+
   int enqueue_step(int rel)
   {
     uint64_t launches = 0;
@@ -1393,7 +1423,7 @@ struct Engine : EngineBase {
     for (auto &w : pws) {
       if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, rel); launches++; }
       if (w.total_e) {
-        k_tfsf_list<T><<<blocks_for(w.le.nsingle + w.le.nmulti, 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
+        k_tfsf_list<T><<<blocks_for(tfsf_threads(w.le), 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
         launches++;
       }
     }
@@ -1415,7 +1445,7 @@ struct Engine : EngineBase {
     for (auto &w : pws) {
       if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
       if (w.total_h) {
-        k_tfsf_list<T><<<blocks_for(w.lh.nsingle + w.lh.nmulti, 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
+        k_tfsf_list<T><<<blocks_for(tfsf_threads(w.lh), 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
         launches++;
       }
     }
@@ -1728,9 +1758,12 @@ extern "C" int vgpu_create(const vgpu_problem *p, vgpu_engine **out)
   if (e != cudaSuccess || ndev == 0) return set_err(VGPU_ENODEV, "no CUDA device: %s", cudaGetErrorString(e));
   int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceProp prop;
-  cudaGetDeviceProperties(&prop, dev);
-  if (prop.major != 10) return set_err(VGPU_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a", dev, prop.major, prop.minor);
+  // Two attributes, not cudaGetDeviceProperties, which queries every
+  // property and costs milliseconds per engine.
+  int major = 0, minor = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  if (major != 10) return set_err(VGPU_ENODEV, "device %d is sm_%d%d; this engine is built for sm_100a", dev, major, minor);
   EngineBase *impl = nullptr;
   int rc;
   if (p->precision == VGPU_FP64) {

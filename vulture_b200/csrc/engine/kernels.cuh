@@ -553,13 +553,22 @@ struct TfsfList {
 };
 
 template <typename T>
-__global__ void k_tfsf_prepare(PwView<T> pw, TfsfView tv, TfsfList<T> tl)
+__global__ void k_tfsf_prepare(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, int efield)
 {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= tl.nentries) return;
   TfsfEntry<T> &en = tl.ent[e];
-  const int c = tv.it[en.q()].inc;
+  const TfsfItem &item = tv.it[en.q()];
+  const int c = item.inc;
   const int i = tl.pos[3 * e], j = tl.pos[3 * e + 1], k = tl.pos[3 * e + 2];
+  // The corrected point's line length and coefficients, as the sweeps read
+  // them (pos holds the incident-field position, shifted along the axis).
+  {
+    const int gi = (item.axis == 0 ? i : item.axis == 1 ? j : k) - item.shift;
+    en.idv = efield ? g.idh[item.axis][gi] : g.ide[item.axis][gi];
+    en.ca = efield ? g.coef(item.c, en.x) : (T)0;
+    en.cb = efield ? g.coef(3 + item.c, en.x) : g.coef(6 + item.c - HX, en.x);
+  }
   if (!pw.use_aux) {
     // Phase term of the analytic incident field (src/planewave.c:450-554):
     // d = kinc . (r - r0), r at the component's node or mid-edge position.
@@ -620,21 +629,37 @@ __device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv,
   return v - en.cb * (en.idv * inc);
 }
 
+// Threads [0, ceil(nsingle / 4)) take four single entries each, spaced
+// ceil(nsingle / 4) apart so each of the four loads is coalesced across the
+// warp, with all loads issued before the first use; the threads after them
+// take one multi-entry run each.
+constexpr int kTfsfPerThread = 4;
+
 template <typename T>
 __global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, double dt,
                             const uint64_t *step_base, int step_rel, int efield)
 {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= tl.nsingle + tl.nmulti) return;
+  const int ns4 = (tl.nsingle + kTfsfPerThread - 1) / kTfsfPerThread;
+  if (t >= ns4 + tl.nmulti) return;
   const uint64_t n = *step_base + step_rel;
   const double time = efield ? n * dt : (n + 0.5) * dt;
-  if (t < tl.nsingle) {
-    const TfsfEntry<T> en = tl.ent[t];
-    T *F = g.F[tv.it[en.q()].c];
-    F[en.x] = tfsf_apply(pw, tv, en, F[en.x], time, efield);
+  if (t < ns4) {
+    TfsfEntry<T> en[kTfsfPerThread];
+    T v[kTfsfPerThread];
+#pragma unroll
+    for (int m = 0; m < kTfsfPerThread; m++)
+      if (t + m * ns4 < tl.nsingle) en[m] = tl.ent[t + m * ns4];
+#pragma unroll
+    for (int m = 0; m < kTfsfPerThread; m++)
+      if (t + m * ns4 < tl.nsingle) v[m] = g.F[tv.it[en[m].q()].c][en[m].x];
+#pragma unroll
+    for (int m = 0; m < kTfsfPerThread; m++)
+      if (t + m * ns4 < tl.nsingle) g.F[tv.it[en[m].q()].c][en[m].x] = tfsf_apply(pw, tv, en[m], v[m], time, efield);
     return;
   }
-  const int e0 = tl.mstart[t - tl.nsingle], e1 = tl.mstart[t - tl.nsingle + 1];
+  const int r = t - ns4;
+  const int e0 = tl.mstart[r], e1 = tl.mstart[r + 1];
   const TfsfEntry<T> first = tl.ent[e0];
   T *F = g.F[tv.it[first.q()].c];
   T v = F[first.x];

@@ -429,14 +429,17 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       gs++;
 
       const int64_t x = x0 + (int64_t)i * g.s0;
-      if (ESWEEP) {
-        if (sel & 1u) F0[x] = cf[0] * v0 + cf[3] * c0;
-        if (sel & 2u) F1[x] = cf[1] * v1 + cf[4] * c1;
-        if (sel & 4u) F2[x] = cf[2] * v2 + cf[5] * c2;
-      } else {
-        if (sel & 1u) F0[x] = v0 + cf[0] * c0;
-        if (sel & 2u) F1[x] = v1 + cf[1] * c1;
-        if (sel & 4u) F2[x] = v2 + cf[2] * c2;
+      // UPML-region tiles hold no bulk points: the branch is uniform.
+      if (!PML || t.bulk) {
+        if (ESWEEP) {
+          if (sel & 1u) F0[x] = cf[0] * v0 + cf[3] * c0;
+          if (sel & 2u) F1[x] = cf[1] * v1 + cf[4] * c1;
+          if (sel & 4u) F2[x] = cf[2] * v2 + cf[5] * c2;
+        } else {
+          if (sel & 1u) F0[x] = v0 + cf[0] * c0;
+          if (sel & 2u) F1[x] = v1 + cf[1] * c1;
+          if (sel & 4u) F2[x] = v2 + cf[2] * c2;
+        }
       }
       if (PML) {
         const T xa = __shfl_sync(0xffffffffu, pa_l, p), xb = __shfl_sync(0xffffffffu, pb_l, p);
