@@ -534,7 +534,7 @@ def main():
     ap.add_argument("--batch-count", type=int, default=32)
     ap.add_argument("--batch-steps", type=int, nargs=2, default=[400, 1600])
     ap.add_argument("--serve-count", type=int, default=24)
-    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-rate", type=float, default=6.0)
     ap.add_argument("--serve-nmax", type=int, default=128)
     ap.add_argument("--serve-steps", type=int, nargs=2, default=[400, 4000])
     ap.add_argument("--serve-budget-gb", type=float, default=8.0)
