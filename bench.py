@@ -40,6 +40,46 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def init_dist(world: int, backend: str = "nccl"):
+    """The process group for N > 1 replicas (None for one process), with a
+    short timeout so ranks that wait for a lost peer end with an error."""
+    if world <= 1:
+        return None
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(value: float, dist, device="cuda") -> float:
+    """The largest of every rank's value; every rank must call it."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, dist, device="cuda") -> float:
+    """The sum of every rank's value; every rank must call it."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_throughput(n_out: int, steps: int, ms_max: float, world: int) -> float:
+    """Whole-job Mcell-updates/s of `world` replicas of n_out cells that each
+    ran `steps` steps, timed by the slowest rank's ms."""
+    return world * n_out * steps / (ms_max * 1e-3) / 1e6
+
+
 def make_mesh(directory: Path, nt: int, plane: int = None) -> Path:
     from vulture_b200 import meshgen
 
@@ -214,12 +254,7 @@ def run_gpu_arm(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dist = init_dist(world)
     import vulture_b200 as vb
     from vulture_b200 import _native as N
 
@@ -248,11 +283,8 @@ def run_gpu_arm(args):
     ms = st.run_ms
     launches = int(st.kernel_launches)
     g.check_finite()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n_out * args.steps / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(ms, dist)
+    value = replica_throughput(n_out, args.steps, ms, world)
 
     # Roofline of the dominant kernel, each sweep timed live on the engine's
     # stream with CUDA events.  Bytes: the algorithmic words of each point
@@ -391,6 +423,7 @@ def run_batch_workload(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
+    dist = init_dist(world)
     rng = __import__("random").Random(4 + rank)
     texts = [meshgen.config4_mesh(rng, q, nmin=32, nmax=160, ntmin=args.batch_steps[0], ntmax=args.batch_steps[1])
              for q in range(args.batch_count)]
@@ -406,6 +439,8 @@ def run_batch_workload(args):
 
     # End to end: engines created on worker threads while the ones before
     # them step (solve_batch), then every solve's observers read back.
+    if dist:
+        dist.barrier()
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
         runs = solve_batch(meshes, "fp32")
@@ -416,6 +451,8 @@ def run_batch_workload(args):
     for r in runs:
         r.close()
     # Stepping alone: all engines created first, then vgpu_run_batch.
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     runs = [vb.GpuRun(m, "fp32") for m in meshes]
     t1 = time.perf_counter()
@@ -427,19 +464,27 @@ def run_batch_workload(args):
         r.close()
     # The plain FP64 path: one solve after another, each created, run to its
     # end and read back.
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for m in meshes:
         g = vb.GpuRun(m, "fp64").run()
         g.td()
         g.close()
     wall64 = time.perf_counter() - t0
+    # Whole job: every rank's solves over the slowest rank's time.
+    wall32, wall64, step_s = (max_over_ranks(v, dist) for v in (wall32, wall64, step_s))
+    solves = sum_over_ranks(len(meshes), dist)
+    nbytes = sum_over_ranks(nbytes, dist)
+    cell_updates = int(sum_over_ranks(cell_updates, dist))
+    launches = int(sum_over_ranks(launches, dist))
     peak, peak_kind = peaks()
     achieved = nbytes / step_s / 1e9
     shutil.rmtree(d, ignore_errors=True)
-    sps32, sps64 = len(meshes) / wall32, len(meshes) / wall64
+    sps32, sps64 = solves / wall32, solves / wall64
     if rank == 0:
         print(json.dumps({
-            "metric": "batched solves/s", "value": sps32 * world, "unit": "solves/s", "n_gpus": world,
+            "metric": "batched solves/s", "value": sps32, "unit": "solves/s", "n_gpus": world,
             "steps": 1, "warmup": 1, "ms_per_step": wall32 * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": f"{len(meshes)} meshes, per-axis 32-160 cells, 6-cell UPML, PEC/dielectric "
@@ -451,16 +496,19 @@ def run_batch_workload(args):
             "mcell_updates_per_s": cell_updates / step_s / 1e6,
             "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
             "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG["fp32"],
-                              "frac": cell_updates / step_s * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9 / peak,
+                              "frac": cell_updates / step_s * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9 / peak / world,
                               "what": "stepping: cell-updates/s x 27 algorithmic words per cell, of measured"},
             "run_batch": {"create_s": create_s, "step_s": step_s},
             "fp64_sequential_solves_per_s": sps64, "speedup_vs_fp64_sequential": sps32 / sps64,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak / world, "traffic": None,
                          "what": "algorithmic sweep bytes of every engine over the batch's stepping time"},
-            "e2e": {"value": sps32 * world, "unit": "solves/s", "wall_s": wall32, "h2d_bytes_per_step": None,
+            "e2e": {"value": sps32, "unit": "solves/s", "wall_s": wall32, "h2d_bytes_per_step": None,
                     "d2h_bytes_per_step": None},
             "gpu_launches": launches, "clocks": clk.summary()}))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_serve_workload(args):
@@ -478,6 +526,7 @@ def run_serve_workload(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
+    dist = init_dist(world)
     rng = random.Random(5 + rank)
     texts = [meshgen.config5_request(rng, q, nmin=48, nmax=args.serve_nmax, ntmin=args.serve_steps[0],
                                      ntmax=args.serve_steps[1]) for q in range(args.serve_count)]
@@ -497,12 +546,22 @@ def run_serve_workload(args):
         done = srv.run(reqs, keep_results=False)
         return srv, done
 
+    if dist:
+        dist.barrier()
     with ClockSampler(local) as clk:
         srv, done = serve("fp32", int(args.serve_budget_gb * 2**30), args.serve_slots)
     s32 = latency_summary(done)
     # Plain FP64: the same stream, one solve at a time.
+    if dist:
+        dist.barrier()
     srv64, done64 = serve("fp64", int(args.serve_budget_gb * 2**30), 1)
     s64 = latency_summary(done64)
+    # Whole job: the worst rank's latencies, every rank's solves/s added.
+    for summ in (s32, s64):
+        for key in ("p50_s", "p99_s", "mean_s"):
+            summ[key] = max_over_ranks(summ[key], dist)
+        summ["solves_per_s"] = sum_over_ranks(summ["solves_per_s"], dist)
+        summ["cell_updates"] = int(sum_over_ranks(summ["cell_updates"], dist))
     shutil.rmtree(d, ignore_errors=True)
     if rank == 0:
         print(json.dumps({
@@ -519,6 +578,9 @@ def run_serve_workload(args):
             "peak_active": srv.peak_active, "peak_budget_bytes": srv.peak_bytes,
             "e2e": {"value": s32["p99_s"], "unit": "s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
             "clocks": clk.summary()}))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
