@@ -14,9 +14,15 @@ reference's own CPU build on the host cores instead.
 """
 from __future__ import annotations
 
+import os
+
+# Before any CUDA context exists: 32 hardware work queues, so the batch and
+# serve workloads' many streams do not share queues (the package sets the
+# same default when it is imported first).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import argparse
 import json
-import os
 import shutil
 import subprocess
 import sys
@@ -289,13 +295,17 @@ def run_gpu_arm(args):
     # Roofline of the dominant kernel, each sweep timed live on the engine's
     # stream with CUDA events.  Bytes: the algorithmic words of each point
     # the launch updates, by the bulk or the UPML formula.
+    # A mesh with UPML regions runs each half step as one launch of the UPML
+    # kernel (bulk, mixed and UPML tiles); the bulk kernel then has no tiles.
     kern = {}
-    for name, kid, wb, wp in (("k_sweep_e_bulk", N.VGPU_K_BULK_E, WORDS_E, WORDS_PML_E),
-                              ("k_sweep_h_bulk", N.VGPU_K_BULK_H, WORDS_H, WORDS_PML_H),
-                              ("k_sweep_e_pml", N.VGPU_K_PML_E, WORDS_E, WORDS_PML_E),
-                              ("k_sweep_h_pml", N.VGPU_K_PML_H, WORDS_H, WORDS_PML_H)):
-        kms, pts = g.time_kernel(kid, warmup=3, iters=20)
+    for name, kid, wb, wp in (("k_sweep_tma<E,bulk>", N.VGPU_K_BULK_E, WORDS_E, WORDS_PML_E),
+                              ("k_sweep_tma<H,bulk>", N.VGPU_K_BULK_H, WORDS_H, WORDS_PML_H),
+                              ("k_sweep_tma<E,UPML>", N.VGPU_K_PML_E, WORDS_E, WORDS_PML_E),
+                              ("k_sweep_tma<H,UPML>", N.VGPU_K_PML_H, WORDS_H, WORDS_PML_H)):
         bp, pp = g.sweep_points(kid)
+        if not bp and not pp:
+            continue
+        kms, pts = g.time_kernel(kid, warmup=3, iters=20)
         nbytes = (wb * bp + wp * pp) / 3.0 * B_ALG[prec]
         kern[name] = dict(ms=kms, cells=pts / 3.0, bulk_points=bp, pml_points=pp, bytes=nbytes,
                           gbs=nbytes / (kms * 1e-3) / 1e9)
@@ -413,9 +423,9 @@ def _sweep_bytes(g, prec):
 def run_batch_workload(args):
     """Many independent meshes of uneven size (seeded PEC/dielectric slabs,
     6-cell UPML, a hard or soft dipole), FP32, solved together (solve_batch:
-    creation on worker threads overlapping the stepping, one stream per
-    engine), against the same meshes solved one after another by the plain
-    FP64 path.  Solves/s counts create + steps + observer read-back."""
+    engines created, then all stepped side by side, one stream per engine),
+    against the same meshes solved one after another by the plain FP64 path.
+    Solves/s counts create + steps + observer read-back."""
     import torch
 
     import vulture_b200 as vb
@@ -437,8 +447,8 @@ def run_batch_workload(args):
 
     from vulture_b200.serve import solve_batch
 
-    # End to end: engines created on worker threads while the ones before
-    # them step (solve_batch), then every solve's observers read back.
+    # End to end: engines created one after another, then stepped together
+    # (solve_batch), then every solve's observers read back.
     if dist:
         dist.barrier()
     with ClockSampler(local) as clk:
@@ -447,6 +457,9 @@ def run_batch_workload(args):
         for r in runs:
             r.td()
         wall32 = time.perf_counter() - t0
+    timeline = {"last_started_s": max(r.batch_started for r in runs),
+                "first_finished_s": min(r.batch_finished for r in runs),
+                "last_finished_s": max(r.batch_finished for r in runs)}
     launches = sum(int(r.stats().kernel_launches) for r in runs)
     for r in runs:
         r.close()
@@ -490,15 +503,14 @@ def run_batch_workload(args):
             "config": {"workload": f"{len(meshes)} meshes, per-axis 32-160 cells, 6-cell UPML, PEC/dielectric "
                                    f"slabs, dipole; {args.batch_steps[0]}-{args.batch_steps[1]} steps each",
                        "cell_updates": cell_updates,
-                       "batch": "solve_batch: engines created on 3 worker threads while earlier ones step, one "
-                                "stream per engine; mcell_updates_per_s from vgpu_run_batch over engines created "
-                                "beforehand"},
+                       "batch": "solve_batch: engines created one after another, then vgpu_run_batch, one "
+                                "stream per engine; mcell_updates_per_s from vgpu_run_batch alone"},
             "mcell_updates_per_s": cell_updates / step_s / 1e6,
             "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
             "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG["fp32"],
                               "frac": cell_updates / step_s * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9 / peak / world,
                               "what": "stepping: cell-updates/s x 27 algorithmic words per cell, of measured"},
-            "run_batch": {"create_s": create_s, "step_s": step_s},
+            "run_batch": {"create_s": create_s, "step_s": step_s}, "solve_batch_timeline": timeline,
             "fp64_sequential_solves_per_s": sps64, "speedup_vs_fp64_sequential": sps32 / sps64,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak / world, "traffic": None,

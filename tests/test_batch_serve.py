@@ -58,7 +58,7 @@ def test_batch_equals_solo(precision):
 def test_solve_batch_equals_solo():
     meshes = [vb.Mesh(p) for p in small_meshes()]
     solo = [vb.GpuRun(m, "fp32").run() for m in meshes]
-    runs = solve_batch(meshes, "fp32", workers=2)
+    runs = solve_batch(meshes, "fp32")
     for m, a, b in zip(meshes, runs, solo):
         assert a.step == m.num_steps
         assert_same_run(m, a, b)

@@ -33,3 +33,63 @@ def test_latency_summary_percentiles_and_rate():
     assert s["p99_s"] == pytest.approx(1.4801, abs=1e-9)
     assert s["solves_per_s"] == pytest.approx(100 / (reqs[-1].completed - reqs[0].arrival))
     assert s["cell_updates"] == 1000
+
+
+class FakeRun:
+    """Stands in for GpuRun on the host: each enqueue advances up to 64
+    steps at once and the stream always reads as drained."""
+    live = 0
+    peak = 0
+
+    def __init__(self, mesh, precision):
+        self.mesh, self.precision, self.step = mesh, precision, 0
+        FakeRun.live += 1
+        FakeRun.peak = max(FakeRun.peak, FakeRun.live)
+
+    def stats(self):
+        class S:
+            device_bytes = 1
+        return S()
+
+    def done(self):
+        return True
+
+    def enqueue(self, n=64):
+        q = min(n, self.mesh.num_steps - self.step)
+        self.step += q
+        return q
+
+    def synchronize(self):
+        return self
+
+    def td(self):
+        return None
+
+    def dft(self):
+        return None
+
+    def close(self):
+        FakeRun.live -= 1
+
+
+def test_server_admits_by_slots_and_budget(monkeypatch):
+    import vulture_b200.serve as serve
+
+    monkeypatch.setattr(serve, "GpuRun", FakeRun)
+    FakeRun.live = FakeRun.peak = 0
+    rng = random.Random(9)
+    texts = [meshgen.config5_request(rng, q, nmin=24, nmax=32, ntmin=100, ntmax=300) for q in range(8)]
+    est = max(footprint_estimate(vb.Mesh(stage_text(t, f"e{q}.mesh")), "fp32") for q, t in enumerate(texts))
+    reqs = [Request(t, arrival=0.0, precision="fp32", tag=str(q)) for q, t in enumerate(texts)]
+    srv = serve.Server(budget_bytes=int(2.5 * est), max_active=4)
+    done = srv.run(reqs)
+    assert [r.tag for r in done] == [str(q) for q in range(8)]
+    assert all(r.completed >= r.admitted >= r.arrival for r in done)
+    assert srv.peak_bytes <= srv.budget and srv.peak_active <= 2 and FakeRun.peak <= 2
+    assert FakeRun.live == 0
+    # First come, first served: admissions follow arrival order.
+    assert [r.admitted for r in done] == sorted(r.admitted for r in done)
+    srv = serve.Server(budget_bytes=10 ** 15, max_active=3)
+    FakeRun.peak = 0
+    srv.run([Request(t, arrival=0.0) for t in texts])
+    assert FakeRun.peak <= 3 and srv.peak_active <= 3

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <map>
 #include <mutex>
@@ -101,6 +102,17 @@ struct BlockCache {
     held[dev] = 0;
   }
 };
+
+// Engines being created at this moment, process-wide: a creation's host
+// threads share the cores with the others'.
+static std::atomic<int> g_creating{ 0 };
+
+static int host_threads()
+{
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int busy = std::max(1, g_creating.load());
+  return std::max(1, std::min(32, hw / busy));
+}
 
 static BlockCache &block_cache()
 {
@@ -255,13 +267,15 @@ struct Engine : EngineBase {
     uint32_t smem = 0;
     uint64_t bulk_points = 0, pml_points = 0;   // field points one launch updates
   };
-  SweepLaunch sw_e[2], sw_h[2];   // [0] bulk tiles, [1] UPML and mixed tiles
+  SweepLaunch sw_e[2], sw_h[2];   // [0] bulk kernel's tiles, [1] UPML kernel's tiles
   SweepMaps maps_e{}, maps_h{};
   PmlFull<T> pfe{}, pfh{};
   int pml_face[6] = {};
   int *d_err = nullptr;
-  cudaStream_t s2 = nullptr;                   // second stream of the sweep pairs
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // Set-up work (uploads, clears, list preparation) runs on a stream of the
+  // device's highest priority: with other engines stepping on the device,
+  // its few small kernels start ahead of their queued sweep blocks.
+  cudaStream_t ss = nullptr;
   // fused sweeps
   CoefIndex cie{}, cih{};
   // graph
@@ -272,7 +286,7 @@ struct Engine : EngineBase {
   {
     if (graph) cudaGraphExecDestroy(graph);
     if (s) cudaStreamSynchronize(s);
-    if (s2) cudaStreamSynchronize(s2);
+    if (ss) cudaStreamSynchronize(ss);
     if (cs) cudaStreamSynchronize(cs);
     mem.free_all();
     if (h_bin) cudaFreeHost(h_bin);
@@ -280,10 +294,8 @@ struct Engine : EngineBase {
       if (ev_fill[q]) cudaEventDestroy(ev_fill[q]);
       if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
     }
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
     if (cs) cudaStreamDestroy(cs);
-    if (s2) cudaStreamDestroy(s2);
+    if (ss) cudaStreamDestroy(ss);
     if (s) cudaStreamDestroy(s);
   }
 
@@ -291,7 +303,7 @@ struct Engine : EngineBase {
   int upload(U **d, const U *h, size_t n)
   {
     if (mem.alloc(d, n)) return VGPU_ENOMEM;
-    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, s));
+    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
     return 0;
   }
 
@@ -302,7 +314,7 @@ struct Engine : EngineBase {
     std::vector<T> tmp(n + pad ? n + pad : 1, (T)0);
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
     if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
-    if (n + pad) CK(cudaMemcpy(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice));
+    if (n + pad) CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
     return 0;
   }
 
@@ -316,7 +328,7 @@ struct Engine : EngineBase {
         T *dst = tmp.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
         for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
       }
-    CK(cudaMemcpy(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice, ss));
     return 0;
   }
 
@@ -343,7 +355,9 @@ struct Engine : EngineBase {
   int create(const vgpu_problem *in)
   {
     PhaseClock pc;
+    g_creating++;
     int rc = create_phases(in, pc);
+    g_creating--;
     pclock = nullptr;
     pc.print(vol);
     return rc;
@@ -360,9 +374,11 @@ struct Engine : EngineBase {
     pclock = &pc;
     p = *in;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    {
+      int least = 0, greatest = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      CK(cudaStreamCreateWithPriority(&ss, cudaStreamNonBlocking, greatest));
+    }
     n2p = (p.n[2] + 31) / 32 * 32;
     g.n0 = p.n[0];
     g.n1 = p.n[1];
@@ -371,7 +387,7 @@ struct Engine : EngineBase {
     g.s0 = (int64_t)p.n[1] * n2p;
     vol = (int64_t)p.n[0] * g.s0;
     if (mem.alloc(&fields, (size_t)vol * 6)) return VGPU_ENOMEM;
-    CK(cudaMemset(fields, 0, sizeof(T) * vol * 6));
+    CK(cudaMemsetAsync(fields, 0, sizeof(T) * vol * 6, ss));
     for (int c = 0; c < 6; c++) g.F[c] = fields + (int64_t)c * vol;
     pc.mark("fields");
     // Coefficients: a one-byte index and a table where the mesh allows it
@@ -399,7 +415,7 @@ struct Engine : EngineBase {
       g.idh[a] = d;
     }
     if (mem.alloc(&d_step, 1)) return VGPU_ENOMEM;
-    CK(cudaMemset(d_step, 0, sizeof(uint64_t)));
+    CK(cudaMemsetAsync(d_step, 0, sizeof(uint64_t), ss));
     pc.mark("coef");
 
     // Bulk limits.
@@ -422,7 +438,7 @@ struct Engine : EngineBase {
     if (int rc = setup_observers()) return rc;
     pc.mark("observers");
     if (int rc = setup_sweeps()) return rc;
-    CK(cudaStreamSynchronize(s));
+    CK(cudaStreamSynchronize(ss));
     CK(cudaGetLastError());
     pc.mark("sweeps");
     stats.device_bytes = mem.bytes;
@@ -524,8 +540,8 @@ struct Engine : EngineBase {
     if (int rc = upload(&d_debye, items.data(), items.size())) return rc;
     if (int rc = upload(&d_dcoef, coefs.data(), coefs.size())) return rc;
     if (mem.alloc(&d_J, jtot) || mem.alloc(&d_lastE, etot)) return VGPU_ENOMEM;
-    CK(cudaMemset(d_J, 0, sizeof(double2) * (jtot ? jtot : 1)));
-    CK(cudaMemset(d_lastE, 0, sizeof(T) * (etot ? etot : 1)));
+    CK(cudaMemsetAsync(d_J, 0, sizeof(double2) * (jtot ? jtot : 1), ss));
+    CK(cudaMemsetAsync(d_lastE, 0, sizeof(T) * (etot ? etot : 1), ss));
     return 0;
   }
 
@@ -584,9 +600,9 @@ struct Engine : EngineBase {
         upload(&d_adjB, adjB.data(), adjB.size()) || upload(&d_zofs, zofs.data(), zofs.size()))
       return VGPU_ENOMEM;
     if (mem.alloc(&d_zeta, z) || mem.alloc(&d_old, faces * 16) || mem.alloc(&d_etan, faces * 4)) return VGPU_ENOMEM;
-    CK(cudaMemset(d_zeta, 0, sizeof(double2) * (z ? z : 1)));
-    CK(cudaMemset(d_old, 0, sizeof(double) * (faces ? faces * 16 : 1)));
-    CK(cudaMemset(d_etan, 0, sizeof(T) * (faces ? faces * 4 : 1)));
+    CK(cudaMemsetAsync(d_zeta, 0, sizeof(double2) * (z ? z : 1), ss));
+    CK(cudaMemsetAsync(d_old, 0, sizeof(double) * (faces ? faces * 16 : 1), ss));
+    CK(cudaMemsetAsync(d_etan, 0, sizeof(T) * (faces ? faces * 4 : 1), ss));
     // Magnetic correction targets (ops arrive sorted by target).
     std::vector<int64_t> tidx, tstart;
     std::vector<int> tcomp;
@@ -690,11 +706,11 @@ struct Engine : EngineBase {
         if (mem.alloc(&v.Eyi, w.aux_nx + 2) || mem.alloc(&v.Hzi, w.aux_nx + 2) || mem.alloc(&v.PPyi, w.aux_npml) ||
             mem.alloc(&v.Pyi, w.aux_npml) || mem.alloc(&v.Bzi, w.aux_npml))
           return VGPU_ENOMEM;
-        CK(cudaMemset(v.Eyi, 0, sizeof(T) * (w.aux_nx + 2)));
-        CK(cudaMemset(v.Hzi, 0, sizeof(T) * (w.aux_nx + 2)));
-        CK(cudaMemset(v.PPyi, 0, sizeof(T) * w.aux_npml));
-        CK(cudaMemset(v.Pyi, 0, sizeof(T) * w.aux_npml));
-        CK(cudaMemset(v.Bzi, 0, sizeof(T) * w.aux_npml));
+        CK(cudaMemsetAsync(v.Eyi, 0, sizeof(T) * (w.aux_nx + 2), ss));
+        CK(cudaMemsetAsync(v.Hzi, 0, sizeof(T) * (w.aux_nx + 2), ss));
+        CK(cudaMemsetAsync(v.PPyi, 0, sizeof(T) * w.aux_npml, ss));
+        CK(cudaMemsetAsync(v.Pyi, 0, sizeof(T) * w.aux_npml, ss));
+        CK(cudaMemsetAsync(v.Bzi, 0, sizeof(T) * w.aux_npml, ss));
         T *d;
         if (upload_real(&d, w.aux_adx, w.aux_npml)) return VGPU_ENOMEM; v.adx = d;
         if (upload_real(&d, w.aux_bdx, w.aux_npml)) return VGPU_ENOMEM; v.bdx = d;
@@ -832,9 +848,9 @@ struct Engine : EngineBase {
     tl.pos = dpos;
     tl.mstart = dm;
     mark("upload");
-    k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, s>>>(g, L.pv, tv, tl, efield ? 1 : 0);
+    k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, ss>>>(g, L.pv, tv, tl, efield ? 1 : 0);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(s));
+    CK(cudaStreamSynchronize(ss));
     mark("prepare");
     return 0;
   }
@@ -852,7 +868,7 @@ struct Engine : EngineBase {
       bool operator<(const Key &o) const { return memcmp(v, o.v, sizeof v) < 0; }
     };
     const int n0 = p.n[0];
-    const int nthr = std::max(1, std::min<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())), n0));
+    const int nthr = std::max(1, std::min<int>(host_threads(), n0));
     std::vector<uint8_t> idx((size_t)vol, 0);
     struct Part {
       std::vector<Key> keys;   // local tuples in first-seen order
@@ -1139,12 +1155,12 @@ struct Engine : EngineBase {
   int setup_sweeps()
   {
     if (mem.alloc(&d_err, 1)) return VGPU_ENOMEM;
-    CK(cudaMemset(d_err, 0, sizeof(int)));
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), ss));
     if (has_pml) {
       if (int rc = check_disjoint()) return rc;
       T *aux = nullptr;
       if (mem.alloc(&aux, (size_t)vol * 9)) return VGPU_ENOMEM;
-      CK(cudaMemset(aux, 0, sizeof(T) * vol * 9));
+      CK(cudaMemsetAsync(aux, 0, sizeof(T) * vol * 9, ss));
       for (int c = 0; c < 6; c++) pfe.aux[c] = aux + (int64_t)c * vol;
       for (int c = 0; c < 3; c++) pfh.aux[c] = aux + (int64_t)(6 + c) * vol;
     }
@@ -1207,6 +1223,22 @@ struct Engine : EngineBase {
               }
               (r ? pml : bulk).push_back(t);
             }
+      }
+      // With UPML regions, one launch of the UPML kernel takes every tile,
+      // bulk tiles interleaved evenly with the UPML and mixed ones: a block's
+      // memory-bound bulk tiles and issue-bound UPML tiles overlap on the SM,
+      // where two launches ran one after the other (config-2 FP32 step 153
+      // -> 148 us).  Bulk tiles load no auxiliaries.
+      if (!pml.empty() && !bulk.empty()) {
+        std::vector<SweepTile> all;
+        all.reserve(bulk.size() + pml.size());
+        const size_t nb = bulk.size(), np = pml.size();
+        for (size_t ib = 0, ip = 0; ib < nb || ip < np;) {
+          if (ip < np && (ib >= nb || ip * (nb + 1) <= ib * (np + 1))) all.push_back(pml[ip++]);
+          else all.push_back(bulk[ib++]);
+        }
+        pml.swap(all);
+        bulk.clear();
       }
       // Narrow boxes must stay narrower than the full ones; else use those.
       wn = (wn + halo - 1) / halo * halo;
@@ -1296,8 +1328,8 @@ struct Engine : EngineBase {
     if (mem.alloc(&d_stage, npc * kTB) || mem.alloc(&d_re, npc * p.num_freq) || mem.alloc(&d_im, npc * p.num_freq) ||
         mem.alloc(&d_tw, (size_t)kTB * p.num_freq))
       return VGPU_ENOMEM;
-    CK(cudaMemset(d_re, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
-    CK(cudaMemset(d_im, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1)));
+    CK(cudaMemsetAsync(d_re, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1), ss));
+    CK(cudaMemsetAsync(d_im, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1), ss));
     if (upload(&d_omega, p.omega, p.num_freq)) return VGPU_ENOMEM;
     return setup_bin();
   }
@@ -1361,23 +1393,12 @@ struct Engine : EngineBase {
 
   static unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
-  // The bulk and UPML sweeps of a half step write disjoint points and read
-  // only the other field, so they run side by side: the UPML launch on a
-  // second stream, forked from and joined back to the engine's stream.
+  // The sweep of a half step: one launch, the UPML kernel over every tile
+  // when the mesh has UPML regions, else the bulk kernel.
   int launch_sweep_pair(bool esweep, uint64_t *count)
   {
-    const SweepLaunch *L = esweep ? sw_e : sw_h;
-    if (!L[0].ntiles || !L[1].ntiles) {
-      if (int rc = launch_sweeps(esweep, 1, count)) return rc;
-      return launch_sweeps(esweep, 0, count);
-    }
-    CK(cudaEventRecord(ev_fork, s));
-    CK(cudaStreamWaitEvent(s2, ev_fork, 0));
-    if (int rc = launch_sweeps(esweep, 1, count, s2)) return rc;
-    if (int rc = launch_sweeps(esweep, 0, count, s)) return rc;
-    CK(cudaEventRecord(ev_join, s2));
-    CK(cudaStreamWaitEvent(s, ev_join, 0));
-    return 0;
+    if (int rc = launch_sweeps(esweep, 1, count)) return rc;
+    return launch_sweeps(esweep, 0, count);
   }
 
   // One time step, in the order of src/simulation.c:156-222, `rel` steps
@@ -1623,7 +1644,9 @@ struct Engine : EngineBase {
   int write_field(int c, const double *in) override
   {
     CK(cudaStreamSynchronize(s));
-    return upload_volume(g.F[c], in);
+    if (int rc = upload_volume(g.F[c], in)) return rc;
+    CK(cudaStreamSynchronize(ss));
+    return 0;
   }
 
   // Launch one sweep over its tile list; with `required` an empty list is an

@@ -18,12 +18,13 @@
 // plane is computed.  Stores go straight to global memory, predicated on
 // the point's update box, one coalesced row per warp.
 //
-// Two kernels per half step.  The bulk kernel takes tiles that hold only
-// bulk points.  The UPML kernel takes the X and Y regions' tiles and the
-// bulk-footprint tiles whose k rows reach into a Z region; each point picks
-// the bulk or the UPML update from the boxes it lies in, so the thin Z
-// slabs ride in the same 32-wide rows as the bulk next to them, with their
-// auxiliaries in narrow boxes over the slab's columns.
+// One launch per half step.  Without UPML regions the bulk kernel (PML =
+// false) takes every tile.  With them the UPML kernel does: the bulk tiles,
+// the X and Y regions' tiles and the bulk-footprint tiles whose k rows reach
+// into a Z region, interleaved; each point picks the bulk or the UPML update
+// from the boxes it lies in, so the thin Z slabs ride in the same 32-wide
+// rows as the bulk next to them, with their auxiliaries in narrow boxes over
+// the slab's columns, and bulk-only tiles load no auxiliaries.
 //
 // Plane bookkeeping: a tile with planes i0..i1 (n planes) uses n + 1
 // stages.  The E sweep marches up: stage 0 holds only Hy, Hz of plane
@@ -280,12 +281,14 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
           for (int c = 1; c < 3; c++)
             tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
         } else {
-          mbar_arrive_expect_tx(bar, tt.ax < 0 ? full_tx : narrow_tx);
+          // Tiles of bulk points only (reg[0] < 0) load no auxiliaries.
+          const bool has_aux = tt.reg[0] >= 0;
+          mbar_arrive_expect_tx(bar, !has_aux ? full_tx - L::NAUX * L::OWN_B : (tt.ax < 0 ? full_tx : narrow_tx));
           for (int c = 0; c < 3; c++)
             tma_load_3d(st + L::OFF_OWN + c * round128(L::OWN_B), &maps.own[c], bar, tt.k0, tt.j0, i);
           for (int c = 0; c < 3; c++)
             tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
-          for (int c = 0; c < L::NAUX; c++) {
+          for (int c = 0; c < (has_aux ? L::NAUX : 0); c++) {
             if (tt.ax < 0)
               tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.aux[c], bar, tt.k0, tt.j0, i);
             else
