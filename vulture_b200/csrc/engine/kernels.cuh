@@ -629,11 +629,12 @@ __device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv,
   return v - en.cb * (en.idv * inc);
 }
 
-// Threads [0, ceil(nsingle / 4)) take four single entries each, spaced
-// ceil(nsingle / 4) apart so each of the four loads is coalesced across the
-// warp, with all loads issued before the first use; the threads after them
-// take one multi-entry run each.
-constexpr int kTfsfPerThread = 4;
+// Threads [0, ceil(nsingle / 2)) take two single entries each, spaced
+// ceil(nsingle / 2) apart so each load is coalesced across the warp, with
+// both loads issued before the first use (two per thread timed faster than
+// one or four on config 2); the threads after them take one multi-entry
+// run each.
+constexpr int kTfsfPerThread = 2;
 
 template <typename T>
 __global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, double dt,
