@@ -249,6 +249,15 @@ typedef struct {
  * on the calling thread first.  Calls on one engine must not overlap. */
 int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
 
+/* Checks on the host, without a device, how the engine would tile the
+ * problem's E and H sweeps: every point of each swept component's bulk and
+ * UPML update boxes must be claimed by exactly one tile and no other point by
+ * any, and every tile must keep the sweep kernel's limits.  *violations
+ * receives the number of failures (0 for a sound plan), *tiles the number of
+ * tiles of both sweeps.  precision selects the storage word (VGPU_FP32 or
+ * VGPU_FP64), which sets the halo alignment. */
+int vgpu_check_sweep_plan(const vgpu_problem *problem, int32_t precision, int64_t *violations, int64_t *tiles);
+
 /* The calling thread's current CUDA device, for hosts without the CUDA
  * runtime of their own (worker threads that create engines for a device). */
 int vgpu_set_device(int32_t device);

@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
         "vgpu_sweep_points": (C.c_int, [P, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "vgpu_enqueue": (C.c_int, [P, C.c_uint64, C.POINTER(C.c_uint64)]),
         "vgpu_set_device": (C.c_int, [C.c_int32]),
+        "vgpu_check_sweep_plan": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "vgpu_get_device": (C.c_int, [C.POINTER(C.c_int32)]),
         "vgpu_query": (C.c_int, [P]),
         "vgpu_synchronize": (C.c_int, [P]),
@@ -118,6 +119,7 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vgpu_current_step", "vgpu_time_kernel", "vgpu_get_stats", "vgpu_destroy", "vgpu_last_error",
            "vgpu_set_bin_sink", "vgpu_dft_accumulate_static", "vhost_num_bin", "vhost_bin_begin", "vhost_bin_sink",
            "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
-           "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device"]
+           "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device",
+           "vgpu_check_sweep_plan"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3

@@ -197,6 +197,145 @@ struct PwLaunch {
   TfsfList<T> le{}, lh{};   // point lists of the E and H corrections
 };
 
+// ---- host-side box helpers and the sweep plan --------------------------
+
+static Box unite(const Box b[3])
+{
+  Box u{ 1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30) };
+  for (int c = 0; c < 3; c++) {
+    if (b[c].empty()) continue;
+    u.i0 = std::min(u.i0, b[c].i0); u.i1 = std::max(u.i1, b[c].i1);
+    u.j0 = std::min(u.j0, b[c].j0); u.j1 = std::max(u.j1, b[c].j1);
+    u.k0 = std::min(u.k0, b[c].k0); u.k1 = std::max(u.k1, b[c].k1);
+  }
+  return u;
+}
+
+static bool boxes_meet(const Box &u, const Box &v)
+{
+  return !u.empty() && !v.empty() && u.i0 <= v.i1 && v.i0 <= u.i1 && u.j0 <= v.j1 && v.j0 <= u.j1 && u.k0 <= v.k1 &&
+         v.k0 <= u.k1;
+}
+
+static int64_t box_overlap(const Box &u, const Box &v)
+{
+  if (!boxes_meet(u, v)) return 0;
+  Box x{ std::max(u.i0, v.i0), std::min(u.i1, v.i1), std::max(u.j0, v.j0),
+         std::min(u.j1, v.j1), std::max(u.k0, v.k0), std::min(u.k1, v.k1) };
+  return x.count();
+}
+
+static Box tile_box(const SweepTile &t)
+{
+  return Box{ t.i0, t.i1, t.j0, t.j0 + kSweepJH - 1, t.k0, t.k0 + kSweepKW - 1 };
+}
+
+// The UPML regions of a problem: region q is outer face face[q], with the
+// update limits lim[q][field] (src/pml.c:44-84).
+struct RegionSet {
+  int nreg = 0;
+  int face[6] = {};
+  Box lim[6][6];
+};
+
+static RegionSet regions_of(const vgpu_problem &p)
+{
+  RegionSet rs;
+  for (int r = 0; r < 6; r++) {
+    if (!p.pml_present[r]) continue;
+    const int q = rs.nreg++;
+    rs.face[q] = r;
+    for (int f = 0; f < 6; f++) rs.lim[q][f] = box_from(p.pml_flim[r][f]);
+  }
+  return rs;
+}
+
+// The tiles of one half step (host only).  Columns of 32 x 8 points, cut
+// into runs of i planes sized so a launch has several tiles per resident
+// block (the pipeline runs across tile boundaries).  Bulk-footprint tiles
+// whose rows reach into a Z region (the thin UPML slabs at the k ends) carry
+// both the bulk box and the Z region; the X and Y regions get their own
+// tiles.  With UPML regions, one launch of the UPML kernel takes every tile,
+// bulk tiles interleaved evenly with the UPML and mixed ones: a block's
+// memory-bound bulk tiles and issue-bound UPML tiles overlap on the SM,
+// where two launches ran one after the other (config-2 FP32 step 153 -> 148
+// us).  halo: elements per 16 bytes of the storage type; nsm: SMs.
+struct SweepPlan {
+  std::vector<SweepTile> bulk, pml;   // the bulk kernel's and the UPML kernel's tiles
+  int wn = 0;                         // width of the narrow auxiliary boxes (0: unused)
+};
+
+static SweepPlan plan_sweep(const Box &ub, const RegionSet &rs, bool es, int halo, int nsm)
+{
+  SweepPlan pl;
+  auto run_len = [&](int64_t cells) {
+    int64_t t = cells / (256LL * nsm * 16);
+    return (int)std::max<int64_t>(4, std::min<int64_t>(kSweepMaxPlanes, t));
+  };
+  std::vector<SweepTile> &bulk = pl.bulk, &pml = pl.pml;
+  int wn = 0;
+  Box zun[2];
+  int zreg[2] = { -1, -1 }, nz = 0;
+  Box core = ub;
+  for (int q = 0; q < rs.nreg; q++) {
+    Box c3[3] = { rs.lim[q][es ? EX : HX], rs.lim[q][es ? EY : HY], rs.lim[q][es ? EZ : HZ] };
+    Box u = unite(c3);
+    if (u.i1 < u.i0) continue;
+    if (rs.face[q] / 2 == 2) {
+      zun[nz] = u;
+      zreg[nz++] = q;
+      if (core.empty()) core = u;
+      core = Box{ std::min(core.i0, u.i0), std::max(core.i1, u.i1), std::min(core.j0, u.j0),
+                  std::max(core.j1, u.j1), std::min(core.k0, u.k0), std::max(core.k1, u.k1) };
+    } else {
+      const int ti = run_len(u.count());
+      for (int i = u.i0; i <= u.i1; i += ti)
+        for (int j = u.j0; j <= u.j1; j += kSweepJH)
+          for (int k = (u.k0 / kSweepKW) * kSweepKW; k <= u.k1; k += kSweepKW)
+            pml.push_back(SweepTile{ { q, -1 }, 0, i, std::min(i + ti - 1, u.i1), j, k, -1 });
+    }
+  }
+  if (!core.empty()) {
+    const int ti = run_len(core.count());
+    for (int i = core.i0; i <= core.i1; i += ti)
+      for (int j = core.j0; j <= core.j1; j += kSweepJH)
+        for (int k = (core.k0 / kSweepKW) * kSweepKW; k <= core.k1; k += kSweepKW) {
+          SweepTile t{ { -1, -1 }, 1, i, std::min(i + ti - 1, core.i1), j, k, -1 };
+          const Box tb = tile_box(t);
+          int r = 0, zi = -1;
+          for (int z = 0; z < nz; z++)
+            if (boxes_meet(tb, zun[z])) {
+              t.reg[r++] = zreg[z];
+              zi = z;
+            }
+          // One Z slab: its auxiliaries in a narrow box over its columns.
+          if (r == 1) {
+            const int ax = std::max(zun[zi].k0, k) & ~(halo - 1);
+            t.ax = ax;
+            wn = std::max(wn, std::min(zun[zi].k1, k + kSweepKW - 1) - ax + 1);
+          }
+          (r ? pml : bulk).push_back(t);
+        }
+  }
+  if (!pml.empty() && !bulk.empty()) {
+    std::vector<SweepTile> all;
+    all.reserve(bulk.size() + pml.size());
+    const size_t nb = bulk.size(), np = pml.size();
+    for (size_t ib = 0, ip = 0; ib < nb || ip < np;) {
+      if (ip < np && (ib >= nb || ip * (nb + 1) <= ib * (np + 1))) all.push_back(pml[ip++]);
+      else all.push_back(bulk[ib++]);
+    }
+    pml.swap(all);
+    bulk.clear();
+  }
+  // Narrow boxes must stay narrower than the full ones; else use those.
+  wn = (wn + halo - 1) / halo * halo;
+  if (wn > kSweepKW)
+    for (SweepTile &t : pml) t.ax = -1;
+  pl.wn = wn > kSweepKW ? 0 : wn;
+  return pl;
+}
+
 template <typename T>
 struct Engine : EngineBase {
   vgpu_problem p{};
@@ -447,17 +586,6 @@ struct Engine : EngineBase {
     return rc;
   }
 
-  static Box unite(const Box b[3])
-  {
-    Box u{ 1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30) };
-    for (int c = 0; c < 3; c++) {
-      if (b[c].empty()) continue;
-      u.i0 = std::min(u.i0, b[c].i0); u.i1 = std::max(u.i1, b[c].i1);
-      u.j0 = std::min(u.j0, b[c].j0); u.j1 = std::max(u.j1, b[c].j1);
-      u.k0 = std::min(u.k0, b[c].k0); u.k1 = std::max(u.k1, b[c].k1);
-    }
-    return u;
-  }
 
   int setup_pml()
   {
@@ -1019,24 +1147,8 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  static bool boxes_meet(const Box &u, const Box &v)
-  {
-    return !u.empty() && !v.empty() && u.i0 <= v.i1 && v.i0 <= u.i1 && u.j0 <= v.j1 && v.j0 <= u.j1 && u.k0 <= v.k1 &&
-           v.k0 <= u.k1;
-  }
 
-  static int64_t box_overlap(const Box &u, const Box &v)
-  {
-    if (!boxes_meet(u, v)) return 0;
-    Box x{ std::max(u.i0, v.i0), std::min(u.i1, v.i1), std::max(u.j0, v.j0),
-           std::min(u.j1, v.j1), std::max(u.k0, v.k0), std::min(u.k1, v.k1) };
-    return x.count();
-  }
 
-  static Box tile_box(const SweepTile &t)
-  {
-    return Box{ t.i0, t.i1, t.j0, t.j0 + kSweepJH - 1, t.k0, t.k0 + kSweepKW - 1 };
-  }
 
   // Per-tile headers (see SweepHeader): membership masks, line lengths and
   // UPML profiles, in the storage type, as the device arrays hold them.
@@ -1164,96 +1276,22 @@ struct Engine : EngineBase {
       for (int c = 0; c < 6; c++) pfe.aux[c] = aux + (int64_t)c * vol;
       for (int c = 0; c < 3; c++) pfh.aux[c] = aux + (int64_t)(6 + c) * vol;
     }
-    // Tiles: 32 x 8 columns, i runs sized so each launch has several tiles
-    // per resident block, for balance; the pipeline runs across tile
-    // boundaries.  Bulk-footprint tiles whose rows reach into a Z region
-    // (the thin UPML slabs at the k ends) go to the UPML kernel with both
-    // the bulk box and the Z region boxes; the X and Y regions get their own
-    // tiles.
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
-    auto run_len = [&](int64_t cells) {
-      int64_t t = cells / (256LL * nsm * 16);
-      return (int)std::max<int64_t>(4, std::min<int64_t>(kSweepMaxPlanes, t));
-    };
     const int halo = 16 / (int)sizeof(T);
+    const RegionSet rs = regions_of(p);
     for (int es = 0; es < 2; es++) {
-      const Box &ub = es ? ube : ubh;
-      std::vector<SweepTile> bulk, pml;
-      int wn = 0;
-      Box zun[2];
-      int zreg[2] = { -1, -1 }, nz = 0;
-      Box core = ub;
-      for (int q = 0; q < pv.nreg; q++) {
-        Box c3[3] = { pv.lim[q][es ? EX : HX], pv.lim[q][es ? EY : HY], pv.lim[q][es ? EZ : HZ] };
-        Box u = unite(c3);
-        if (u.i1 < u.i0) continue;
-        if (pml_face[q] / 2 == 2) {
-          zun[nz] = u;
-          zreg[nz++] = q;
-          if (core.empty()) core = u;
-          core = Box{ std::min(core.i0, u.i0), std::max(core.i1, u.i1), std::min(core.j0, u.j0),
-                      std::max(core.j1, u.j1), std::min(core.k0, u.k0), std::max(core.k1, u.k1) };
-        } else {
-          const int ti = run_len(u.count());
-          for (int i = u.i0; i <= u.i1; i += ti)
-            for (int j = u.j0; j <= u.j1; j += kSweepJH)
-              for (int k = (u.k0 / kSweepKW) * kSweepKW; k <= u.k1; k += kSweepKW)
-                pml.push_back(SweepTile{ { q, -1 }, 0, i, std::min(i + ti - 1, u.i1), j, k, -1 });
-        }
-      }
-      if (!core.empty()) {
-        const int ti = run_len(core.count());
-        for (int i = core.i0; i <= core.i1; i += ti)
-          for (int j = core.j0; j <= core.j1; j += kSweepJH)
-            for (int k = (core.k0 / kSweepKW) * kSweepKW; k <= core.k1; k += kSweepKW) {
-              SweepTile t{ { -1, -1 }, 1, i, std::min(i + ti - 1, core.i1), j, k, -1 };
-              const Box tb = tile_box(t);
-              int r = 0, zi = -1;
-              for (int z = 0; z < nz; z++)
-                if (boxes_meet(tb, zun[z])) {
-                  t.reg[r++] = zreg[z];
-                  zi = z;
-                }
-              // One Z slab: its auxiliaries in a narrow box over its columns.
-              if (r == 1) {
-                const int ax = std::max(zun[zi].k0, k) & ~(halo - 1);
-                t.ax = ax;
-                wn = std::max(wn, std::min(zun[zi].k1, k + kSweepKW - 1) - ax + 1);
-              }
-              (r ? pml : bulk).push_back(t);
-            }
-      }
-      // With UPML regions, one launch of the UPML kernel takes every tile,
-      // bulk tiles interleaved evenly with the UPML and mixed ones: a block's
-      // memory-bound bulk tiles and issue-bound UPML tiles overlap on the SM,
-      // where two launches ran one after the other (config-2 FP32 step 153
-      // -> 148 us).  Bulk tiles load no auxiliaries.
-      if (!pml.empty() && !bulk.empty()) {
-        std::vector<SweepTile> all;
-        all.reserve(bulk.size() + pml.size());
-        const size_t nb = bulk.size(), np = pml.size();
-        for (size_t ib = 0, ip = 0; ib < nb || ip < np;) {
-          if (ip < np && (ib >= nb || ip * (nb + 1) <= ib * (np + 1))) all.push_back(pml[ip++]);
-          else all.push_back(bulk[ib++]);
-        }
-        pml.swap(all);
-        bulk.clear();
-      }
-      // Narrow boxes must stay narrower than the full ones; else use those.
-      wn = (wn + halo - 1) / halo * halo;
-      if (wn > kSweepKW)
-        for (SweepTile &t : pml) t.ax = -1;
-      (es ? maps_e : maps_h).wn = wn > kSweepKW ? 0 : wn;
+      SweepPlan pl = plan_sweep(es ? ube : ubh, rs, es != 0, halo, nsm);
+      (es ? maps_e : maps_h).wn = pl.wn;
       SweepLaunch *L = es ? sw_e : sw_h;
       const bool comp = (es ? cie : cih).idx != nullptr;
       mark("tiles");
       if (es) {
-        if (int rc = prepare_launch<true, false>(L[0], bulk, comp)) return rc;
-        if (int rc = prepare_launch<true, true>(L[1], pml, comp)) return rc;
+        if (int rc = prepare_launch<true, false>(L[0], pl.bulk, comp)) return rc;
+        if (int rc = prepare_launch<true, true>(L[1], pl.pml, comp)) return rc;
       } else {
-        if (int rc = prepare_launch<false, false>(L[0], bulk, comp)) return rc;
-        if (int rc = prepare_launch<false, true>(L[1], pml, comp)) return rc;
+        if (int rc = prepare_launch<false, false>(L[0], pl.bulk, comp)) return rc;
+        if (int rc = prepare_launch<false, true>(L[1], pl.pml, comp)) return rc;
       }
       mark("headers");
     }
@@ -1803,6 +1841,63 @@ extern "C" int vgpu_create(const vgpu_problem *p, vgpu_engine **out)
     return rc;
   }
   *out = new vgpu_engine{ impl, dev };
+  return 0;
+}
+
+// Host-only check of the sweep plan: each swept component's bulk and UPML
+// points are claimed by exactly one tile and no other point is; tiles keep
+// the kernel's limits (planes, k alignment, narrow auxiliary boxes that
+// cover the UPML points of their tile).
+extern "C" int vgpu_check_sweep_plan(const vgpu_problem *p, int32_t precision, int64_t *violations, int64_t *tiles)
+{
+  if (!p || !violations || !tiles) return set_err(VGPU_EINVAL, "null argument");
+  if (int rc = validate(p)) return rc;
+  const int halo = precision == VGPU_FP64 ? 2 : 4;
+  const int n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
+  const RegionSet rs = regions_of(*p);
+  int64_t bad = 0, ntiles = 0;
+  std::vector<uint8_t> claims((size_t)n0 * n1 * n2);
+  for (int es = 0; es < 2; es++) {
+    Box bb[3];
+    for (int c = 0; c < 3; c++) bb[c] = box_from(p->gfilim[(es ? 0 : 3) + c]);
+    const SweepPlan pl = plan_sweep(unite(bb), rs, es != 0, halo, 148);
+    std::vector<SweepTile> all(pl.bulk);
+    all.insert(all.end(), pl.pml.begin(), pl.pml.end());
+    ntiles += (int64_t)all.size();
+    for (const SweepTile &t : all) {
+      if (t.i1 - t.i0 + 1 > kSweepMaxPlanes || t.i1 < t.i0 || t.k0 % kSweepKW) bad++;
+      if (t.ax >= 0 && (t.ax % halo || pl.wn <= 0)) bad++;
+    }
+    for (int c = 0; c < 3; c++) {
+      const int f = (es ? EX : HX) + c;
+      std::fill(claims.begin(), claims.end(), 0);
+      for (const SweepTile &t : all) {
+        const Box tb = tile_box(t);
+        for (int i = std::max(tb.i0, 0); i <= std::min(tb.i1, n0 - 1); i++)
+          for (int j = std::max(tb.j0, 0); j <= std::min(tb.j1, n1 - 1); j++)
+            for (int k = std::max(tb.k0, 0); k <= std::min(tb.k1, n2 - 1); k++) {
+              int n = (t.bulk && bb[c].contains(i, j, k)) ? 1 : 0;
+              for (int r = 0; r < 2; r++) {
+                if (t.reg[r] < 0 || !rs.lim[t.reg[r]][f].contains(i, j, k)) continue;
+                n++;
+                if (t.ax >= 0 && (k < t.ax || k >= t.ax + pl.wn)) bad++;   // auxiliaries not loaded
+              }
+              uint8_t &cl = claims[((size_t)i * n1 + j) * n2 + k];
+              cl = (uint8_t)std::min(255, cl + n);
+            }
+      }
+      for (int i = 0; i < n0; i++)
+        for (int j = 0; j < n1; j++)
+          for (int k = 0; k < n2; k++) {
+            int want = bb[c].contains(i, j, k) ? 1 : 0;
+            for (int q = 0; q < rs.nreg; q++) want += rs.lim[q][f].contains(i, j, k) ? 1 : 0;
+            if (want > 1) want = -1;   // overlapping boxes: the engine refuses such problems
+            if (want >= 0 && claims[((size_t)i * n1 + j) * n2 + k] != want) bad++;
+          }
+    }
+  }
+  *violations = bad;
+  *tiles = ntiles;
   return 0;
 }
 
