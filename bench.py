@@ -93,7 +93,7 @@ def make_mesh(directory: Path, nt: int, plane: int = None) -> Path:
     kw["nt"] = nt
     if plane is not None:
         kw["plane"] = plane
-    return Path(meshgen.write(meshgen.config2(seed=2, **kw), directory / "config2.mesh"))
+    return Path(meshgen.write(meshgen.graded_upml(seed=2, **kw), directory / "graded_upml.mesh"))
 
 
 class ClockSampler:
@@ -171,7 +171,7 @@ def time_reference(binary: str, mesh_dir: Path, nt_lo: int, nt_hi: int, threads:
         make_mesh(d, nt, plane)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         t0 = time.perf_counter()
-        r = subprocess.run([binary, "-n", str(threads), "config2.mesh"], cwd=d, env=env, capture_output=True,
+        r = subprocess.run([binary, "-n", str(threads), "graded_upml.mesh"], cwd=d, env=env, capture_output=True,
                            text=True)
         walls.append(time.perf_counter() - t0)
         if r.returncode != 0:
@@ -179,7 +179,7 @@ def time_reference(binary: str, mesh_dir: Path, nt_lo: int, nt_hi: int, threads:
         if n_out is None:
             import vulture_b200 as vb
 
-            n_out = vb.Mesh(d / "config2.mesh").num_cells
+            n_out = vb.Mesh(d / "graded_upml.mesh").num_cells
         shutil.rmtree(d, ignore_errors=True)
     dt = walls[1] - walls[0]
     return n_out * (nt_hi - nt_lo) / dt / 1e6, walls
@@ -209,7 +209,7 @@ def run_reference_arm(args):
     shutil.rmtree(work, ignore_errors=True)
     base.update({"value": value, "ms_per_step": 5170176 / (value * 1e6) * 1e3,
                  "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
-                                  "sample": f"config-2 mesh, vulture_ref_f32_omp -n {threads}, runs of {w} and "
+                                  "sample": f"graded 200x160x120 UPML mesh, vulture_ref_f32_omp -n {threads}, runs of {w} and "
                                             f"{w + k} steps, difference of wall times {walls}"},
                  "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
                          "d2h_bytes_per_step": 0}})
@@ -359,7 +359,7 @@ def run_gpu_arm(args):
                 v, walls = time_reference(str(binary), cw, 5, 45, threads)
                 v2, walls2 = time_reference(str(binary), cw, 5, 45, threads, plane=0)
                 cpu = {"value": v, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
-                       "sample": f"config-2 mesh on vulture_ref_f32_omp -n {threads}: runs of 5 and 45 steps, "
+                       "sample": f"graded 200x160x120 UPML mesh on vulture_ref_f32_omp -n {threads}: runs of 5 and 45 steps, "
                                  f"difference of wall times {[round(x, 2) for x in walls]} s",
                        "without_fd_plane": v2}
             except Exception as exc:  # the baseline is reported, never required
@@ -435,7 +435,7 @@ def run_batch_workload(args):
     torch.cuda.set_device(local)
     dist = init_dist(world)
     rng = __import__("random").Random(4 + rank)
-    texts = [meshgen.config4_mesh(rng, q, nmin=32, nmax=160, ntmin=args.batch_steps[0], ntmax=args.batch_steps[1])
+    texts = [meshgen.batch_mesh(rng, q, nmin=32, nmax=160, ntmin=args.batch_steps[0], ntmax=args.batch_steps[1])
              for q in range(args.batch_count)]
     d, paths = _meshes_dir(texts, "vb_batch_")
     meshes = [vb.Mesh(p) for p in paths]
@@ -540,7 +540,7 @@ def run_serve_workload(args):
     torch.cuda.set_device(local)
     dist = init_dist(world)
     rng = random.Random(5 + rank)
-    texts = [meshgen.config5_request(rng, q, nmin=48, nmax=args.serve_nmax, ntmin=args.serve_steps[0],
+    texts = [meshgen.serving_request(rng, q, nmin=48, nmax=args.serve_nmax, ntmin=args.serve_steps[0],
                                      ntmax=args.serve_steps[1]) for q in range(args.serve_count)]
     arrivals, t = [], 0.0
     for _ in texts:
@@ -604,7 +604,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=["config2", "batch", "serve"])
+    ap.add_argument("--workload", default="graded", choices=["graded", "batch", "serve"])
     ap.add_argument("--batch-count", type=int, default=32)
     ap.add_argument("--batch-steps", type=int, nargs=2, default=[400, 1600])
     ap.add_argument("--serve-count", type=int, default=24)

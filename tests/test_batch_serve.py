@@ -20,8 +20,8 @@ pytestmark = pytest.mark.gpu
 
 def small_meshes():
     rng = random.Random(41)
-    texts = [meshgen.config4_mesh(rng, q, nmin=20, nmax=40, ntmin=150, ntmax=260) for q in range(4)]
-    texts.append(meshgen.config2(nt=90, dims=(40, 32, 24), plane=8, nfreq=12, npml=4, ntd=4))
+    texts = [meshgen.batch_mesh(rng, q, nmin=20, nmax=40, ntmin=150, ntmax=260) for q in range(4)]
+    texts.append(meshgen.graded_upml(nt=90, dims=(40, 32, 24), plane=8, nfreq=12, npml=4, ntd=4))
     return [stage_text(t, f"b{q}.mesh") for q, t in enumerate(texts)]
 
 
@@ -96,7 +96,7 @@ def test_batch_rejects_overrun_of_a_listed_twice_engine():
 
 def test_served_results_equal_solo_and_budget_queues():
     rng = random.Random(5)
-    texts = [meshgen.config5_request(rng, q, nmin=24, nmax=40, ntmin=120, ntmax=200) for q in range(6)]
+    texts = [meshgen.serving_request(rng, q, nmin=24, nmax=40, ntmin=120, ntmax=200) for q in range(6)]
     meshes = [vb.Mesh(stage_text(t, f"s{q}.mesh")) for q, t in enumerate(texts)]
     ests = [footprint_estimate(m, "fp32") for m in meshes]
     reqs = [Request(t, arrival=0.002 * q, precision="fp32", tag=str(q)) for q, t in enumerate(texts)]

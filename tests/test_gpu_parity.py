@@ -111,11 +111,11 @@ def many_media_mesh(nmedia=300, seed=5):
 def synthetic():
     rng = random.Random(11)
     return {
-        "config1_full": meshgen.config1(),
-        "config2_short": meshgen.config2(nt=130, dims=(200, 160, 120), plane=16, nfreq=20),
-        "config3_small": meshgen.config3(nt=150, dims=(80, 64, 56), plane=8, nfreq=20),
-        "config4_mesh": meshgen.config4_mesh(rng, 0, nmin=32, nmax=64, ntmin=200, ntmax=300),
-        "config5_req": meshgen.config5_request(rng, 0, nmin=48, nmax=64, ntmin=200, ntmax=300),
+        "pec_cube_full": meshgen.pec_cube(),
+        "graded_upml_short": meshgen.graded_upml(nt=130, dims=(200, 160, 120), plane=16, nfreq=20),
+        "shielded_enclosure_small": meshgen.shielded_enclosure(nt=150, dims=(80, 64, 56), plane=8, nfreq=20),
+        "batch_mesh": meshgen.batch_mesh(rng, 0, nmin=32, nmax=64, ntmin=200, ntmax=300),
+        "serving_request": meshgen.serving_request(rng, 0, nmin=48, nmax=64, ntmin=200, ntmax=300),
         "many_media": many_media_mesh(),
     }
 
@@ -125,7 +125,7 @@ def test_synthetic_workloads_fp64_equal_oracle(name):
     m, g, c = solve_both(stage_text(synthetic()[name]), "fp64")
     # The analytic plane-wave incident field uses CUDA's exp/sin/cos on the
     # device and glibc's in the oracle: values agree to 1e-12 relative.
-    if name in ("config2_short", "config3_small") or ("PW " in synthetic()[name]):
+    if name in ("graded_upml_short", "shielded_enclosure_small") or ("PW " in synthetic()[name]):
         assert max_rel(g.td().reshape(-1, 6), c.td().reshape(-1, 6)) <= 1e-12
     else:
         assert_same(m, g, c)

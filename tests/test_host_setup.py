@@ -27,7 +27,7 @@ def test_reference_parser_negative_cases_fail(name):
 def test_time_step_formula():
     """dt = CN / c0 / sqrt(sum 1/dmin^2) over primary and secondary edges (src/grid.c:673-675)."""
     n = 16
-    m = vb.Mesh(stage_text(meshgen.config1(nt=10, n=n)))
+    m = vb.Mesh(stage_text(meshgen.pec_cube(nt=10, n=n)))
     c0 = 299792458.0
     lines = [i * 0.01 for i in range(n + 1)]
     de = [lines[i + 1] - lines[i] for i in range(n)]
@@ -37,7 +37,7 @@ def test_time_step_formula():
 
 
 def test_outer_cell_count_includes_pml():
-    m = vb.Mesh(stage_text(meshgen.config2(nt=10, dims=(20, 16, 12), plane=2, nfreq=4, ntd=1)))
+    m = vb.Mesh(stage_text(meshgen.graded_upml(nt=10, dims=(20, 16, 12), plane=2, nfreq=4, ntd=1)))
     assert m.num_cells == (20 + 16) * (16 + 16) * (12 + 16)
 
 

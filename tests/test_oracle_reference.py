@@ -52,11 +52,11 @@ def test_oracle_equals_reference_fp64(case):
 def synthetic_small():
     rng = random.Random(7)
     return {
-        "config1": meshgen.config1(nt=60, n=20),
-        "config2": meshgen.config2(nt=80, dims=(30, 24, 20), plane=4, nfreq=12, ntd=3),
-        "config3": meshgen.config3(nt=60, dims=(40, 32, 28), plane=4, nfreq=10),
-        "config4": meshgen.config4_mesh(rng, 0, nmin=16, nmax=28, ntmin=50, ntmax=80),
-        "config5": meshgen.config5_request(rng, 1, nmin=20, nmax=28, ntmin=50, ntmax=80),
+        "pec_cube": meshgen.pec_cube(nt=60, n=20),
+        "graded_upml": meshgen.graded_upml(nt=80, dims=(30, 24, 20), plane=4, nfreq=12, ntd=3),
+        "shielded_enclosure": meshgen.shielded_enclosure(nt=60, dims=(40, 32, 28), plane=4, nfreq=10),
+        "batch_mesh": meshgen.batch_mesh(rng, 0, nmin=16, nmax=28, ntmin=50, ntmax=80),
+        "serving_request": meshgen.serving_request(rng, 1, nmin=20, nmax=28, ntmin=50, ntmax=80),
     }
 
 

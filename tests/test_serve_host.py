@@ -12,8 +12,8 @@ from helpers import stage_text
 
 def test_footprint_grows_with_cells_and_word_size():
     rng = random.Random(3)
-    small = vb.Mesh(stage_text(meshgen.config5_request(rng, 0, nmin=24, nmax=24, ntmin=100, ntmax=100), "a.mesh"))
-    big = vb.Mesh(stage_text(meshgen.config5_request(rng, 1, nmin=48, nmax=48, ntmin=100, ntmax=100), "b.mesh"))
+    small = vb.Mesh(stage_text(meshgen.serving_request(rng, 0, nmin=24, nmax=24, ntmin=100, ntmax=100), "a.mesh"))
+    big = vb.Mesh(stage_text(meshgen.serving_request(rng, 1, nmin=48, nmax=48, ntmin=100, ntmax=100), "b.mesh"))
     for m in (small, big):
         # At least the six field volumes and the engine's fixed blocks.
         assert footprint_estimate(m, "fp32") > m.num_cells * 6 * 4 + (64 << 20)
@@ -78,7 +78,7 @@ def test_server_admits_by_slots_and_budget(monkeypatch):
     monkeypatch.setattr(serve, "GpuRun", FakeRun)
     FakeRun.live = FakeRun.peak = 0
     rng = random.Random(9)
-    texts = [meshgen.config5_request(rng, q, nmin=24, nmax=32, ntmin=100, ntmax=300) for q in range(8)]
+    texts = [meshgen.serving_request(rng, q, nmin=24, nmax=32, ntmin=100, ntmax=300) for q in range(8)]
     est = max(footprint_estimate(vb.Mesh(stage_text(t, f"e{q}.mesh")), "fp32") for q, t in enumerate(texts))
     reqs = [Request(t, arrival=0.0, precision="fp32", tag=str(q)) for q, t in enumerate(texts)]
     srv = serve.Server(budget_bytes=int(2.5 * est), max_active=4)

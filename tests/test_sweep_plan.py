@@ -39,10 +39,10 @@ def test_reference_meshes_are_tiled_exactly_once(case):
 def synthetic():
     rng = random.Random(11)
     return {
-        "config2_small": meshgen.config2(nt=10, dims=(60, 44, 37), plane=8, nfreq=4, npml=8, ntd=4),
-        "config3_small": meshgen.config3(nt=10, dims=(70, 52, 45), plane=8, nfreq=4),
-        **{f"config4_{q}": meshgen.config4_mesh(rng, q, nmin=32, nmax=80, ntmin=10, ntmax=20) for q in range(4)},
-        **{f"config5_{q}": meshgen.config5_request(rng, q, nmin=48, nmax=70, ntmin=10, ntmax=20) for q in range(4)},
+        "graded_upml_small": meshgen.graded_upml(nt=10, dims=(60, 44, 37), plane=8, nfreq=4, npml=8, ntd=4),
+        "shielded_enclosure_small": meshgen.shielded_enclosure(nt=10, dims=(70, 52, 45), plane=8, nfreq=4),
+        **{f"batch_mesh_{q}": meshgen.batch_mesh(rng, q, nmin=32, nmax=80, ntmin=10, ntmax=20) for q in range(4)},
+        **{f"serving_request_{q}": meshgen.serving_request(rng, q, nmin=48, nmax=70, ntmin=10, ntmax=20) for q in range(4)},
     }
 
 

@@ -258,8 +258,9 @@ static RegionSet regions_of(const vgpu_problem &p)
 // tiles.  With UPML regions, one launch of the UPML kernel takes every tile,
 // bulk tiles interleaved evenly with the UPML and mixed ones: a block's
 // memory-bound bulk tiles and issue-bound UPML tiles overlap on the SM,
-// where two launches ran one after the other (config-2 FP32 step 153 -> 148
-// us).  halo: elements per 16 bytes of the storage type; nsm: SMs.
+// where two launches ran one after the other (graded 200x160x120 UPML mesh,
+// FP32: step 153 -> 148 us).  halo: elements per 16 bytes of the storage
+// type; nsm: SMs.
 struct SweepPlan {
   std::vector<SweepTile> bulk, pml;   // the bulk kernel's and the UPML kernel's tiles
   int wn = 0;                         // width of the narrow auxiliary boxes (0: unused)

