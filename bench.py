@@ -571,7 +571,7 @@ def run_serve_workload(args):
     # Whole job: the worst rank's latencies, every rank's solves/s added.
     for summ in (s32, s64):
         for key in ("p50_s", "p99_s", "mean_s"):
-            summ[key] = max_over_ranks(summ[key], dist)
+            summ[key] = max_over_ranks(summ[key] if summ[key] is not None else float("inf"), dist)
         summ["solves_per_s"] = sum_over_ranks(summ["solves_per_s"], dist)
         summ["cell_updates"] = int(sum_over_ranks(summ["cell_updates"], dist))
     shutil.rmtree(d, ignore_errors=True)

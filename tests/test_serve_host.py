@@ -93,3 +93,21 @@ def test_server_admits_by_slots_and_budget(monkeypatch):
     FakeRun.peak = 0
     srv.run([Request(t, arrival=0.0) for t in texts])
     assert FakeRun.peak <= 3 and srv.peak_active <= 3
+
+
+def test_server_fails_a_bad_request_and_serves_the_rest(monkeypatch):
+    import vulture_b200.serve as serve
+
+    monkeypatch.setattr(serve, "GpuRun", FakeRun)
+    FakeRun.live = FakeRun.peak = 0
+    rng = random.Random(12)
+    good = [meshgen.serving_request(rng, q, nmin=24, nmax=28, ntmin=100, ntmax=150) for q in range(3)]
+    bad = "VM 1.0.0\nDM 8 8 8\nNOT A CARD\nEN\n"
+    reqs = [Request(good[0], 0.0, tag="a"), Request(bad, 0.0, tag="bad"), Request(good[1], 0.0, tag="b"),
+            Request(good[2], 0.0, tag="c")]
+    done = serve.Server(budget_bytes=10 ** 15, max_active=2).run(reqs)
+    errors = {r.tag: r.error for r in done}
+    assert errors["bad"] is not None and all(errors[t] is None for t in "abc")
+    assert FakeRun.live == 0
+    s = latency_summary(done)
+    assert s["failed"] == 1 and s["cell_updates"] > 0

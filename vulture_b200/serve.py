@@ -46,6 +46,7 @@ class Request:
     dft: tuple | None = None
     device_bytes: int = 0         # the engine's own count once created
     estimate: int = 0             # the admission estimate
+    error: str | None = None      # why the solve failed (bad mesh, engine error); None if it ran
 
     @property
     def latency(self) -> float:
@@ -103,8 +104,16 @@ class Server:
         self.peak_bytes = 0
         self.peak_active = 0
 
+    @staticmethod
+    def _fail(r: Request, exc: BaseException, t0: float):
+        r.error = f"{type(exc).__name__}: {exc}"
+        r.completed = time.perf_counter() - t0
+
     def run(self, requests, keep_results: bool = True):
-        """Serve the requests (sorted by arrival); returns them completed."""
+        """Serve the requests (sorted by arrival); returns them completed.
+        A request whose mesh does not parse, or whose engine cannot be
+        created or reports a device error, completes with `error` set; the
+        others are not affected."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending = deque(reqs)
         waiting: deque = deque()      # arrived, not admitted: [request, parse future]
@@ -131,10 +140,15 @@ class Server:
                 for w in list(waiting)[: self.workers]:
                     if w[1] is None:
                         w[1] = pool.submit(parse, w[0])
-                # Admission, first come first served.
+                # Admission, first come first served.  A mesh that fails to
+                # parse fails its request only.
                 while (waiting and waiting[0][1] is not None and waiting[0][1].done()
                        and len(active) + len(creating) < self.max_active):
                     r, fut = waiting[0]
+                    if fut.exception() is not None:
+                        waiting.popleft()
+                        self._fail(r, fut.exception(), t0)
+                        continue
                     mesh, path, est = fut.result()
                     if (active or creating) and used + est > self.budget:
                         break
@@ -149,7 +163,15 @@ class Server:
                 progressed = False
                 still_creating = []
                 for r, mesh, path, fut in creating:
-                    if fut.done():
+                    if fut.done() and fut.exception() is not None:
+                        # The engine could not be created (device memory, a
+                        # problem the engine refuses): this request fails.
+                        self._fail(r, fut.exception(), t0)
+                        mesh.close()
+                        os.unlink(path)
+                        used -= r.estimate
+                        progressed = True
+                    elif fut.done():
                         run = fut.result()
                         r.device_bytes = int(run.stats().device_bytes)
                         r.started = time.perf_counter() - t0
@@ -165,7 +187,16 @@ class Server:
                         still.append((r, mesh, run, path))
                         continue
                     if run.step >= mesh.num_steps:
-                        run.synchronize()
+                        try:
+                            run.synchronize()
+                        except N.NativeError as exc:   # a device-side failure of this solve
+                            self._fail(r, exc, t0)
+                            run.close()
+                            mesh.close()
+                            os.unlink(path)
+                            used -= r.estimate
+                            progressed = True
+                            continue
                         r.completed = time.perf_counter() - t0
                         r.cell_updates = mesh.num_cells * mesh.num_steps
                         if keep_results:
@@ -177,9 +208,18 @@ class Server:
                         used -= r.estimate
                         progressed = True
                         continue
-                    for _ in range(self.max_inflight):
-                        if not run.enqueue(self.block_steps):
-                            break
+                    try:
+                        for _ in range(self.max_inflight):
+                            if not run.enqueue(self.block_steps):
+                                break
+                    except N.NativeError as exc:
+                        self._fail(r, exc, t0)
+                        run.close()
+                        mesh.close()
+                        os.unlink(path)
+                        used -= r.estimate
+                        progressed = True
+                        continue
                     progressed = True
                     still.append((r, mesh, run, path))
                 active = still
@@ -241,10 +281,16 @@ def solve_batch(meshes, precision: str = "fp32"):
 
 
 def latency_summary(reqs):
-    """p50 / p99 latency (arrival to completion), mean, completed solves/s."""
-    lat = np.array([r.latency for r in reqs])
-    span = max(r.completed for r in reqs) - min(r.arrival for r in reqs)
+    """p50 / p99 latency (arrival to completion), mean and solves/s over the
+    requests that ran; failed requests are counted apart."""
+    ok = [r for r in reqs if r.error is None]
+    failed = len(reqs) - len(ok)
+    if not ok:
+        return {"p50_s": None, "p99_s": None, "mean_s": None, "solves_per_s": 0.0, "cell_updates": 0,
+                "failed": failed}
+    lat = np.array([r.latency for r in ok])
+    span = max(r.completed for r in ok) - min(r.arrival for r in ok)
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()),
-            "solves_per_s": len(reqs) / span if span > 0 else float("inf"),
-            "cell_updates": int(sum(r.cell_updates for r in reqs))}
+            "solves_per_s": len(ok) / span if span > 0 else float("inf"),
+            "cell_updates": int(sum(r.cell_updates for r in ok)), "failed": failed}
