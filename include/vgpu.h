@@ -249,8 +249,8 @@ typedef struct {
  * on the calling thread first.  Calls on one engine must not overlap. */
 int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
 
-/* Checks on the host, without a device, how the engine would tile the
- * problem's E and H sweeps: every point of each swept component's bulk and
+/* No counterpart in the reference.  Checks on the host, without a device,
+ * how the engine would tile the problem's E and H sweeps: every point of each swept component's bulk and
  * UPML update boxes must be claimed by exactly one tile and no other point by
  * any, and every tile must keep the sweep kernel's limits.  *violations
  * receives the number of failures (0 for a sound plan), *tiles the number of
@@ -258,8 +258,9 @@ int vgpu_create(const vgpu_problem *problem, vgpu_engine **engine);
  * VGPU_FP64), which sets the halo alignment. */
 int vgpu_check_sweep_plan(const vgpu_problem *problem, int32_t precision, int64_t *violations, int64_t *tiles);
 
-/* The calling thread's current CUDA device, for hosts without the CUDA
- * runtime of their own (worker threads that create engines for a device). */
+/* No counterpart in the reference.  The calling thread's current CUDA
+ * device, for hosts without the CUDA runtime of their own (worker threads
+ * that create engines for a device). */
 int vgpu_set_device(int32_t device);
 int vgpu_get_device(int32_t *device);
 
@@ -285,10 +286,11 @@ typedef void (*vgpu_bin_sink)(void *user, uint64_t first_row, uint32_t num_rows,
 int vgpu_set_bin_sink(vgpu_engine *engine, vgpu_bin_sink sink, void *user);
 
 /* Asynchronous stepping, for callers that keep several engines busy on one
- * device (batches, services).  vgpu_enqueue queues at most max_steps more
- * steps -- one 64-step graph, or single steps up to the next 64-step
- * boundary, never past the problem's last step -- on the engine's stream and
- * returns without waiting; *queued receives the count (0 once the problem is
+ * device (batches, services); the reference runs one mesh per process and
+ * has no counterpart.  vgpu_enqueue queues at most max_steps more steps --
+ * one 64-step block (four launches of the 16-step graph), or single steps up
+ * to the next 64-step boundary, never past the problem's last step -- on the
+ * engine's stream and returns without waiting; *queued receives the count (0 once the problem is
  * done).  Observer folding and binary-row delivery happen as in vgpu_run.
  * vgpu_query returns 1 when the queued work has finished, 0 if not;
  * vgpu_synchronize waits for it and reports any device-side failure. */
@@ -320,10 +322,12 @@ int vgpu_check_finite(vgpu_engine *engine);
 
 uint64_t vgpu_current_step(const vgpu_engine *engine);
 
-/* Sweep kernels of one time step, for vgpu_time_kernel: the launch over
- * tiles holding only bulk points, and the launch over the UPML regions'
- * tiles (the X and Y regions' own, plus the bulk-footprint tiles whose rows
- * reach into a Z region, which update bulk and UPML points together). */
+/* Sweep launches of one time step, for vgpu_time_kernel and
+ * vgpu_sweep_points.  Without UPML regions the bulk kernel's launch takes
+ * every tile of a half step.  With them the UPML kernel's launch does (bulk
+ * tiles, the X and Y regions' tiles, and the bulk-footprint tiles whose rows
+ * reach into a Z region), and the bulk kernel's launch is empty: its point
+ * counts are 0 and timing it is an error. */
 enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 };
 
 /* Field points one sweep kernel updates per launch with the bulk formula
