@@ -1552,9 +1552,10 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  // Queue the next block of at most max_steps steps (one captured graph, or
-  // single steps up to the next 64-step boundary) on the engine's stream,
-  // with the block's DFT fold and binary-row copy; *queued gets the count.
+  // Queue the next block of at most max_steps steps (four launches of the
+  // 16-step graph, or single steps up to the next 64-step boundary) on the
+  // engine's stream, with the block's DFT fold and binary-row copy; *queued
+  // gets the count.
   int issue_block(uint64_t max_steps, uint64_t *queued)
   {
     const uint64_t n0 = step;
