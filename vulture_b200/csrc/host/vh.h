@@ -253,6 +253,11 @@ typedef struct vhost vh_ctx;
 int vh_fail(vh_ctx *c, const char *fmt, ...);
 void vh_log(vh_ctx *c, int verbose_only, const char *fmt, ...);
 
+/* Grid volumes of n doubles (the coefficient arrays): bytes mapped, and
+ * their release. */
+size_t vh_volume_bytes(size_t n);
+void vh_free_volume(double *p, size_t n);
+
 /* Runs fn(ctx, lo, hi) over [begin, end) split into contiguous ranges on
  * up to 16 threads; one call on the calling thread when work (the points
  * the whole range touches) is small.  The ranges must touch disjoint

@@ -316,24 +316,30 @@ static void paint_range(void *ctx, int lo, int hi)
   }
 }
 
-static void zero_range(void *ctx, int lo, int hi)
-{
-  memset((char *)ctx + ((size_t)lo << 21), 0, (size_t)(hi - lo) << 21);
-}
-
-/* A zeroed volume of n doubles: 2 MiB aligned and advised for huge pages,
- * zeroed by several threads, so first touch costs few page faults. */
-static double *alloc_volume(size_t n)
+size_t vh_volume_bytes(size_t n)
 {
   const size_t huge = (size_t)1 << 21;
-  const size_t bytes = (n * sizeof(double) + huge - 1) / huge * huge;
-  void *p = NULL;
-  if (posix_memalign(&p, huge, bytes ? bytes : huge)) return NULL;
+  return n ? (n * sizeof(double) + huge - 1) / huge * huge : huge;
+}
+
+/* A zeroed volume of n doubles: anonymous pages, which the kernel hands out
+ * zeroed on first touch (the painting threads touch them in parallel), so
+ * nothing writes the volume twice; advised for huge pages.  Freed by
+ * vh_free_volume. */
+static double *alloc_volume(size_t n)
+{
+  const size_t bytes = vh_volume_bytes(n);
+  void *p = mmap(NULL, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+  if (p == MAP_FAILED) return NULL;
 #ifdef MADV_HUGEPAGE
   madvise(p, bytes, MADV_HUGEPAGE);
 #endif
-  vh_parallel_for(0, (int)(bytes / huge), (int64_t)(bytes / sizeof(double)), zero_range, p);
   return p;
+}
+
+void vh_free_volume(double *p, size_t n)
+{
+  if (p) munmap(p, vh_volume_bytes(n));
 }
 
 /* Paint a medium's coefficients over a box (src/grid.c:1726-1873). */

@@ -382,7 +382,7 @@ void vhost_free(vhost *c)
     free(c->pml_ibd[a]); free(c->pml_ibh[a]);
     free(c->pos_node[a]); free(c->pos_half[a]);
   }
-  for (int q = 0; q < 9; q++) free(c->coef[q]);
+  for (int q = 0; q < 9; q++) vh_free_volume(c->coef[q], (size_t)c->n[0] * c->n[1] * c->n[2]);
   for (int m = 0; m < c->num_media; m++) {
     free(c->media[m].res); free(c->media[m].pole); free(c->media[m].dalpha); free(c->media[m].dbeta);
   }
