@@ -111,3 +111,31 @@ def test_server_fails_a_bad_request_and_serves_the_rest(monkeypatch):
     assert FakeRun.live == 0
     s = latency_summary(done)
     assert s["failed"] == 1 and s["cell_updates"] > 0
+
+
+def test_solve_batch_waves_fit_the_budget(monkeypatch):
+    import vulture_b200.serve as serve
+
+    monkeypatch.setattr(serve, "GpuRun", FakeRun)
+
+    def fake_run_batch(runs):
+        for r in runs:
+            while r.enqueue(64):
+                pass
+    monkeypatch.setattr(serve, "run_batch", fake_run_batch)
+    FakeRun.live = FakeRun.peak = 0
+    rng = random.Random(13)
+    meshes = [vb.Mesh(stage_text(meshgen.batch_mesh(rng, q, nmin=16, nmax=24, ntmin=50, ntmax=90), f"w{q}.mesh"))
+              for q in range(7)]
+    est = [footprint_estimate(m, "fp32") for m in meshes]
+    seen = []
+    out = serve.solve_batch(meshes, "fp32", budget_bytes=int(2.5 * max(est)),
+                            on_done=lambda q, r: seen.append((q, r.step == meshes[q].num_steps)))
+    assert out is None
+    assert sorted(q for q, _ in seen) == list(range(7)) and all(ok for _, ok in seen)
+    assert FakeRun.peak <= 2 and FakeRun.live == 0
+    FakeRun.peak = 0
+    runs = serve.solve_batch(meshes, "fp32")
+    assert len(runs) == 7 and FakeRun.peak == 7
+    for r in runs:
+        r.close()

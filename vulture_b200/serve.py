@@ -249,7 +249,7 @@ class Server:
         return reqs
 
 
-def solve_batch(meshes, precision: str = "fp32"):
+def solve_batch(meshes, precision: str = "fp32", budget_bytes: int | None = None, on_done=None):
     """Solve independent meshes to their last step on the current device.
 
     The engines are created one after another, then advanced together by
@@ -259,25 +259,54 @@ def solve_batch(meshes, precision: str = "fp32"):
     overlapped with stepping: both were measured, and engine creations that
     run beside other creations or beside stepping engines wait on each
     other's device allocations and copies (32 engines: 0.17 s one after
-    another, 1.3-1.7 s on three threads).  Returns the finished GpuRun
-    objects in the meshes' order, their results ready to read; each carries
-    batch_started (all engines created) and batch_finished, seconds from the
-    call."""
+    another, 1.3-1.7 s on three threads).
+
+    Without budget_bytes every mesh is solved in one wave and the finished
+    GpuRun objects are returned in the meshes' order, their results ready to
+    read; each carries batch_started (its wave's engines created) and
+    batch_finished, seconds from the call.  With budget_bytes, meshes are
+    taken in order into waves whose footprint estimates fit the budget (a
+    mesh larger than the budget forms a wave alone); on_done(index, run) is
+    called for each finished solve of a wave, after which the engine is
+    closed to make room for the next wave, and the call returns None."""
     t0 = time.perf_counter()
-    runs = []
-    try:
-        for m in meshes:
-            runs.append(GpuRun(m, precision))
-    except BaseException:
-        for r in runs:
-            r.close()
-        raise
-    started = time.perf_counter() - t0
-    run_batch(runs)
-    finished = time.perf_counter() - t0
-    for r in runs:
-        r.batch_started, r.batch_finished = started, finished
-    return runs
+    if budget_bytes is None:
+        waves = [list(range(len(meshes)))]
+    else:
+        waves, cur, used = [], [], 0
+        for q, m in enumerate(meshes):
+            est = footprint_estimate(m, precision)
+            if cur and used + est > budget_bytes:
+                waves.append(cur)
+                cur, used = [], 0
+            cur.append(q)
+            used += est
+        if cur:
+            waves.append(cur)
+    result = [None] * len(meshes)
+    for wave in waves:
+        runs = []
+        try:
+            for q in wave:
+                runs.append(GpuRun(meshes[q], precision))
+        except BaseException:
+            for r in runs:
+                r.close()
+            raise
+        started = time.perf_counter() - t0
+        run_batch(runs)
+        finished = time.perf_counter() - t0
+        for q, r in zip(wave, runs):
+            r.batch_started, r.batch_finished = started, finished
+            if budget_bytes is None:
+                result[q] = r
+                continue
+            try:
+                if on_done is not None:
+                    on_done(q, r)
+            finally:
+                r.close()
+    return result if budget_bytes is None else None
 
 
 def latency_summary(reqs):
