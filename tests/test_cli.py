@@ -19,20 +19,20 @@ def cli(*args, cwd=None):
     return subprocess.run([str(EXE), *args], cwd=cwd, capture_output=True, text=True, timeout=120)
 
 
-def test_help_and_version_exit_zero():
-    r = cli("-h")
+def test_help_and_version_exit_zero(tmp_path):
+    r = cli("-h", cwd=tmp_path)
     assert r.returncode == 0 and "Usage" in r.stdout + r.stderr
-    r = cli("-V")
+    r = cli("-V", cwd=tmp_path)
     assert r.returncode == 0 and "0.7.1" in r.stdout + r.stderr
 
 
-def test_bad_option_exits_one():
-    r = cli("-Z")
+def test_bad_option_exits_one(tmp_path):
+    r = cli("-Z", cwd=tmp_path)
     assert r.returncode == 1 and "invalid option" in r.stdout + r.stderr
 
 
 def test_missing_mesh_exits_six(tmp_path):
-    r = cli(str(tmp_path / "absent.mesh"))
+    r = cli(str(tmp_path / "absent.mesh"), cwd=tmp_path)
     assert r.returncode == 6 and "Cannot open input mesh file" in r.stdout + r.stderr
 
 
