@@ -240,6 +240,17 @@ typedef struct {
   uint64_t steps;             /* steps in that run */
   uint64_t kernel_launches;   /* engine kernels launched in that run */
   uint64_t device_bytes;      /* device memory held by the engine */
+  uint64_t h2d_bytes;         /* bytes copied host->device since creation (problem upload, writes) */
+  /* Stability check, no counterpart in the reference (whose only guard is
+   * the Courant check, src/simulation.c:64-84): FP64 sums of squares of the
+   * E and of the H components over every stored point, computed on the
+   * device at every 64-step boundary and at the problem's last step, as of
+   * energy_step (0: not yet computed).  Not the physical energy (no
+   * permittivity, permeability or cell-volume weights); it grows without
+   * bound when the update is unstable.  vgpu_run and vgpu_synchronize return
+   * VGPU_ENONFINITE when it is not finite. */
+  double energy_e, energy_h;
+  uint64_t energy_step;
 } vgpu_stats;
 
 /* Create an engine on the current CUDA device (cuda:0 unless the caller set
@@ -288,12 +299,13 @@ int vgpu_set_bin_sink(vgpu_engine *engine, vgpu_bin_sink sink, void *user);
 /* Asynchronous stepping, for callers that keep several engines busy on one
  * device (batches, services); the reference runs one mesh per process and
  * has no counterpart.  vgpu_enqueue queues at most max_steps more steps --
- * one 64-step block (four launches of the 16-step graph), or single steps up
- * to the next 64-step boundary, never past the problem's last step -- on the
+ * up to the next 64-step boundary, never past the problem's last step,
+ * replayed from captured step graphs of 16, 8, 4, 2 and 1 steps -- on the
  * engine's stream and returns without waiting; *queued receives the count (0 once the problem is
  * done).  Observer folding and binary-row delivery happen as in vgpu_run.
- * vgpu_query returns 1 when the queued work has finished, 0 if not;
- * vgpu_synchronize waits for it and reports any device-side failure. */
+ * vgpu_query returns 1 when the queued work has finished, 0 if it has
+ * not, and VGPU_ECUDA when the engine's stream reports a device error;
+ * vgpu_synchronize waits for the work and reports any device-side failure. */
 int vgpu_enqueue(vgpu_engine *engine, uint64_t max_steps, uint64_t *queued);
 int vgpu_query(vgpu_engine *engine);
 int vgpu_synchronize(vgpu_engine *engine);
@@ -301,7 +313,9 @@ int vgpu_synchronize(vgpu_engine *engine);
 /* Advance n engines of one device by steps[i] each: their blocks are queued
  * round-robin on the engines' own streams, so the device runs them side by
  * side; returns when all have finished.  The batched form of vgpu_run; each
- * engine's results are the ones vgpu_run would give it alone. */
+ * engine's results are the ones vgpu_run would give it alone.  If queueing
+ * fails for one engine, no further blocks are queued, every engine's queued
+ * work is still waited for, and the first error is returned. */
 int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint64_t *steps);
 
 /* Copy time-domain samples to the host: out[(s*num_td + p)*6 + c] for the
@@ -330,15 +344,27 @@ uint64_t vgpu_current_step(const vgpu_engine *engine);
  * counts are 0 and timing it is an error. */
 enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 };
 
+/* The other parts of a time step, in their order within the step
+ * (src/simulation.c:156-222), and the DFT fold of one 64-step block
+ * (src/observer.c:857-899), for vgpu_time_kernel.  Each part is the launch
+ * (or launches: one per source or plane wave) of that update in the step;
+ * timing a part the problem does not have is an error. */
+enum {
+  VGPU_K_OBSERVE = 4, VGPU_K_BIN_OBSERVE = 5, VGPU_K_MUR_E = 6, VGPU_K_DEBYE = 7, VGPU_K_SIBC_E = 8,
+  VGPU_K_SOURCES_E = 9, VGPU_K_TFSF_E = 10, VGPU_K_GHOST_E = 11, VGPU_K_MUR_H = 12, VGPU_K_SIBC_H = 13,
+  VGPU_K_SOURCES_H = 14, VGPU_K_TFSF_H = 15, VGPU_K_GHOST_H = 16, VGPU_K_DFT_BLOCK = 17
+};
+
 /* Field points one sweep kernel updates per launch with the bulk formula
  * and with the UPML formula. */
 int vgpu_sweep_points(const vgpu_engine *engine, int32_t kernel, uint64_t *bulk_points, uint64_t *pml_points);
 
-/* Profiling hook: launch one of the step's kernels `iters` times on the
- * engine's stream (after `warmup` untimed launches) and report the mean
- * device time per launch from CUDA events, plus the number of field points
- * that kernel updates per launch.  It advances the fields it updates, so
- * call it only when the run's results are no longer needed. */
+/* Profiling hook: launch one of the step's kernels (VGPU_K_*) `iters`
+ * times on the engine's stream (after `warmup` untimed launches) and report
+ * the mean device time per launch from CUDA events, plus the number of field
+ * points a sweep updates per launch (0 for the other parts).  It advances
+ * the state it updates, so call it only when the run's results are no
+ * longer needed. */
 int vgpu_time_kernel(vgpu_engine *engine, int32_t kernel, int32_t warmup, int32_t iters, double *ms_per_launch,
                      uint64_t *points);
 int vgpu_get_stats(const vgpu_engine *engine, vgpu_stats *stats);
@@ -355,16 +381,29 @@ void vgpu_destroy(vgpu_engine *engine);
  * device pointers owned by the caller.  It calls no cudaMalloc or cudaFree:
  * its twiddle table is a file-scope __device__ array of
  * VGPU_STATIC_DFT_MAX_ENTRIES double2 (1 MiB), held on every GPU that loads
- * the library until exit, and rows * freqs beyond that, or more than
- * VGPU_STATIC_DFT_MAX_ROWS rows, are rejected with VGPU_EINVAL.  The first
+ * the library until exit, and rows * freqs beyond that, more than
+ * VGPU_STATIC_DFT_MAX_ROWS rows or more than VGPU_STATIC_DFT_MAX_SERIES
+ * series (8 series per block row of the launch grid, at most 65535 rows) are
+ * rejected with VGPU_EINVAL.  The first
  * call on a device looks up the table's device address; make that call
  * before any stream capture.  Calls share the one table, so calls that
  * overlap on the GPU race; each call runs on the default stream and returns
  * after it has finished. */
 #define VGPU_STATIC_DFT_MAX_ENTRIES 65536
 #define VGPU_STATIC_DFT_MAX_ROWS 256
+#define VGPU_STATIC_DFT_MAX_SERIES (65535 * 8)
 int vgpu_dft_accumulate_static(const double *samples, int32_t num_series, int32_t num_rows, const double *omega,
                                int32_t num_freq, double dt, uint64_t first_step, double *re, double *im);
+
+/* No counterpart in the reference.  Test hook for the failure path of the
+ * sweeps: the number of polls a sweep's compute warps make on a stage's data
+ * barrier before they give up (0: give up at once; a negative value restores
+ * the default bound of about a second).  A sweep whose wait runs out records
+ * it, its blocks wait for their loads in flight and leave, later sweep
+ * launches of the engine skip their work, and vgpu_run returns
+ * VGPU_ETIMEOUT.  The setting belongs to the current device and holds for
+ * every engine on it; change it only while none of them is stepping. */
+int vgpu_set_sweep_wait_limit(int64_t polls);
 
 /* Message of the last error on this thread. */
 const char *vgpu_last_error(void);

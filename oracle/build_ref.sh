@@ -3,7 +3,8 @@
 # oracle's strengthener.  This is test infrastructure: only tests/, the smoke
 # check and the CPU-baseline leg of bench.py execute the binaries it makes.
 #
-# The sources are read where they lie (REF=/root/reference by default).  The
+# The sources are read where they lie: $VULTURE_REF, by default a checkout
+# named `reference` beside this repository.  The
 # FP64 variants need three edits to the reference, so those are built from a
 # patched copy in a temporary directory outside the repository; nothing from
 # the reference is ever written into the repository.  Outputs go to
@@ -24,8 +25,8 @@
 # with WITH_SIBC, minus mur.c which surface.c:42 #includes.
 set -euo pipefail
 
-REF="${VULTURE_REF:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${VULTURE_REF:-$HERE/../../reference}"
 OUT="$HERE/_ref"
 mkdir -p "$OUT"
 

@@ -19,7 +19,7 @@ import shutil
 import sys
 from pathlib import Path
 
-REF = Path(os.environ.get("VULTURE_REF", "/root/reference")) / "tests"
+REF = Path(os.environ.get("VULTURE_REF", str(Path(__file__).resolve().parents[3] / "reference"))) / "tests"
 HERE = Path(__file__).resolve().parent
 
 GOLDEN_CASES = [

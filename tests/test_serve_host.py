@@ -139,3 +139,75 @@ def test_solve_batch_waves_fit_the_budget(monkeypatch):
     assert len(runs) == 7 and FakeRun.peak == 7
     for r in runs:
         r.close()
+
+
+class FaultyRun(FakeRun):
+    """A FakeRun whose stream reports a device error once it has stepped: the
+    fault of a real engine surfaces from vgpu_query as VGPU_ECUDA."""
+
+    def done(self):
+        from vulture_b200 import _native as N
+
+        if self.step > 0:
+            raise N.NativeError(N.VGPU_ECUDA, "stream query: an illegal memory access was encountered")
+        return True
+
+
+def test_server_ends_a_solve_whose_stream_reports_a_device_error(monkeypatch):
+    import vulture_b200.serve as serve
+
+    created = []
+
+    def make(mesh, precision):
+        # The second request's engine fails on the device; the others run.
+        r = (FaultyRun if len(created) == 1 else FakeRun)(mesh, precision)
+        created.append(r)
+        return r
+
+    monkeypatch.setattr(serve, "GpuRun", make)
+    FakeRun.live = FakeRun.peak = 0
+    rng = random.Random(21)
+    texts = [meshgen.serving_request(rng, q, nmin=24, nmax=28, ntmin=100, ntmax=150) for q in range(3)]
+    reqs = [Request(t, 0.0, tag=str(q)) for q, t in enumerate(texts)]
+    done = serve.Server(budget_bytes=10 ** 15, max_active=1).run(reqs)
+    errors = {r.tag: r.error for r in done}
+    assert errors["1"] is not None and "illegal memory access" in errors["1"]
+    assert errors["0"] is None and errors["2"] is None
+    assert all(r.completed is not None for r in done)
+    assert FakeRun.live == 0
+
+
+def test_solve_batch_closes_every_engine_when_the_batch_or_callback_fails(monkeypatch):
+    import vulture_b200.serve as serve
+
+    monkeypatch.setattr(serve, "GpuRun", FakeRun)
+    rng = random.Random(22)
+    meshes = [vb.Mesh(stage_text(meshgen.batch_mesh(rng, q, nmin=16, nmax=20, ntmin=50, ntmax=60), f"f{q}.mesh"))
+              for q in range(4)]
+
+    def failing_batch(runs):
+        raise RuntimeError("device error while stepping")
+
+    monkeypatch.setattr(serve, "run_batch", failing_batch)
+    FakeRun.live = 0
+    with pytest.raises(RuntimeError):
+        serve.solve_batch(meshes, "fp32")
+    assert FakeRun.live == 0
+    with pytest.raises(RuntimeError):
+        serve.solve_batch(meshes, "fp32", budget_bytes=10 ** 15)
+    assert FakeRun.live == 0
+
+    def fake_run_batch(runs):
+        for r in runs:
+            while r.enqueue(64):
+                pass
+
+    monkeypatch.setattr(serve, "run_batch", fake_run_batch)
+
+    def bad_callback(q, r):
+        if q == 1:
+            raise ValueError("callback failed")
+
+    with pytest.raises(ValueError):
+        serve.solve_batch(meshes, "fp32", budget_bytes=10 ** 15, on_done=bad_callback)
+    assert FakeRun.live == 0

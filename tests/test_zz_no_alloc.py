@@ -78,3 +78,6 @@ def test_static_dft_rejects_sizes_beyond_its_table():
     assert "maximum" in N.lib().vgpu_last_error().decode()
     assert f(p, 1, 256, p, 1000, 1e-12, 0, p, p) == N.VGPU_EINVAL
     assert "static twiddle table" in N.lib().vgpu_last_error().decode()
+    # More series than the launch grid's 65535 block rows of 8 hold.
+    assert f(p, 65535 * 8 + 1, 1, p, 1, 1e-12, 0, p, p) == N.VGPU_EINVAL
+    assert "series" in N.lib().vgpu_last_error().decode()

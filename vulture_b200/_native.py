@@ -26,7 +26,8 @@ VGPU_ECANCELLED = -7
 
 class VgpuStats(C.Structure):
     _fields_ = [("run_ms", C.c_double), ("steps", C.c_uint64), ("kernel_launches", C.c_uint64),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64), ("energy_e", C.c_double),
+                ("energy_h", C.c_double), ("energy_step", C.c_uint64)]
 
 
 # void sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows)
@@ -90,6 +91,7 @@ def lib() -> C.CDLL:
         "vgpu_query": (C.c_int, [P]),
         "vgpu_synchronize": (C.c_int, [P]),
         "vgpu_run_batch": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(C.c_uint64)]),
+        "vgpu_set_sweep_wait_limit": (C.c_int, [C.c_int64]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
     }
@@ -120,6 +122,12 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vgpu_set_bin_sink", "vgpu_dft_accumulate_static", "vhost_num_bin", "vhost_bin_begin", "vhost_bin_sink",
            "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
            "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device",
-           "vgpu_check_sweep_plan"]
+           "vgpu_check_sweep_plan", "vgpu_set_sweep_wait_limit"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3
+# Other parts of a step and the 64-step DFT fold, for vgpu_time_kernel.
+STEP_KERNELS = {
+    "k_observe": 4, "k_bin_observe": 5, "k_mur_e": 6, "k_debye": 7, "k_sibc_e": 8, "k_source(E)": 9,
+    "k_tfsf(E)": 10, "k_ghost(E)": 11, "k_mur_h": 12, "k_sibc_h": 13, "k_source(H)": 14, "k_tfsf(H)": 15,
+    "k_ghost(H)": 16, "dft_fold_64": 17,
+}

@@ -91,14 +91,16 @@ def build_oracle() -> Path:
 
 
 def build_reference() -> bool:
-    """Compile the reference solver into oracle/_ref when its sources exist here."""
-    ref = Path(os.environ.get("VULTURE_REF", "/root/reference"))
+    """Compile the reference solver into oracle/_ref when its sources exist:
+    VULTURE_REF, else a checkout named `reference` beside the repository."""
+    ref = Path(os.environ.get("VULTURE_REF", str(ROOT.parent / "reference")))
     if not (ref / "src").is_dir():
         return False
     want = ROOT / "oracle" / "_ref" / "vulture_oracle_f64_dump"
     if want.exists():
         return True
-    _run(["bash", ROOT / "oracle" / "build_ref.sh"])
+    subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh")], check=True, capture_output=True,
+                   env=dict(os.environ, VULTURE_REF=str(ref)))
     return True
 
 

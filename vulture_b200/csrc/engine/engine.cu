@@ -3,8 +3,8 @@
 // vgpu_create uploads a vgpu_problem into device memory (fields and
 // coefficients as padded [n0][n1][n2p] volumes, k rows aligned to 32
 // elements), builds the launch plan of one time step in the reference's order
-// (src/simulation.c:156-222), and captures a chunk of steps in a CUDA graph.
-// vgpu_run replays the graph; the running DFT of the frequency-domain
+// (src/simulation.c:156-222), and captures runs of steps in CUDA graphs.
+// vgpu_run replays the graphs; the running DFT of the frequency-domain
 // observers is accumulated every chunk from a buffer of field samples.
 #include <cmath>
 #include <cstdarg>
@@ -17,6 +17,7 @@
 #include <chrono>
 #include <map>
 #include <mutex>
+#include <string>
 #include <thread>
 
 #include "kernels.cuh"
@@ -47,7 +48,7 @@ extern "C" const char *vgpu_last_error(void) { return g_err; }
 
 static const int kChunk = 64;      // steps per block and per DFT block
 static const int kTB = kChunk;     // DFT staging rows
-static const int kGraphSteps = 16; // steps per captured graph; a block launches it kChunk / kGraphSteps times
+static const int kGraphSteps = 16; // steps of the longest step graph; a full block replays it kChunk / kGraphSteps times
 
 // The device step counter moves once per block of steps; kernels inside
 // the block add their step's offset (step_rel).
@@ -412,19 +413,25 @@ struct Engine : EngineBase {
   PmlFull<T> pfe{}, pfh{};
   int pml_face[6] = {};
   int *d_err = nullptr;
+  // FP64 sums of squares of E and H (k_energy), queued at every 64-step
+  // boundary and at the problem's last step; energy_step is the step of the
+  // latest one queued (0: none yet).
+  double *d_energy = nullptr;
+  uint64_t energy_step = 0;
   // Set-up work (uploads, clears, list preparation) runs on a stream of the
   // device's highest priority: with other engines stepping on the device,
   // its few small kernels start ahead of their queued sweep blocks.
   cudaStream_t ss = nullptr;
   // fused sweeps
   CoefIndex cie{}, cih{};
-  // graph
-  cudaGraphExec_t graph = nullptr;
+  // step graphs (capture_graph)
+  cudaGraphExec_t graphs[5] = {};
   uint64_t launches_per_step = 0;
 
   ~Engine() override
   {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (cudaGraphExec_t gx : graphs)
+      if (gx) cudaGraphExecDestroy(gx);
     if (s) cudaStreamSynchronize(s);
     if (ss) cudaStreamSynchronize(ss);
     if (cs) cudaStreamSynchronize(cs);
@@ -444,6 +451,7 @@ struct Engine : EngineBase {
   {
     if (mem.alloc(d, n)) return VGPU_ENOMEM;
     if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
+    stats.h2d_bytes += sizeof(U) * n;
     return 0;
   }
 
@@ -455,6 +463,7 @@ struct Engine : EngineBase {
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
     if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
     if (n + pad) CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
+    stats.h2d_bytes += sizeof(T) * (n + pad);
     return 0;
   }
 
@@ -469,6 +478,7 @@ struct Engine : EngineBase {
         for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
       }
     CK(cudaMemcpyAsync(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice, ss));
+    stats.h2d_bytes += sizeof(T) * vol;
     return 0;
   }
 
@@ -1267,8 +1277,9 @@ struct Engine : EngineBase {
 
   int setup_sweeps()
   {
-    if (mem.alloc(&d_err, 1)) return VGPU_ENOMEM;
+    if (mem.alloc(&d_err, 1) || mem.alloc(&d_energy, 2)) return VGPU_ENOMEM;
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), ss));
+    CK(cudaMemsetAsync(d_energy, 0, 2 * sizeof(double), ss));
     if (has_pml) {
       if (int rc = check_disjoint()) return rc;
       T *aux = nullptr;
@@ -1440,79 +1451,155 @@ struct Engine : EngineBase {
     return launch_sweeps(esweep, 0, count);
   }
 
-  // One time step, in the order of src/simulation.c:156-222, `rel` steps
-  // past the device step counter.
+  // Threads of one k_tfsf_list launch.
   static int64_t tfsf_threads(const TfsfList<T> &l)
   {
     return (l.nsingle + kTfsfPerThread - 1) / kTfsfPerThread + l.nmulti;
   }
 
+  // The parts of one time step, in the order of src/simulation.c:156-222.
+  // launch_part queues one part `rel` steps past the device step counter
+  // (nothing when the problem has no such work) and counts its kernels.
+  enum Part {
+    P_OBSERVE, P_BIN, P_MUR_E, P_SWEEP_E, P_DEBYE, P_SIBC_E, P_SRC_E, P_TFSF_E, P_GHOST_E,
+    P_MUR_H, P_SWEEP_H, P_SIBC_H, P_SRC_H, P_TFSF_H, P_GHOST_H, P_COUNT
+  };
+
+  bool part_present(int part) const
+  {
+    switch (part) {
+      case P_OBSERVE: return p.num_td || p.num_fd;
+      case P_BIN: return p.num_bin > 0;
+      case P_MUR_E: return mve.nitems > 0;
+      case P_SWEEP_E: return sw_e[0].ntiles || sw_e[1].ntiles;
+      case P_DEBYE: return n_debye > 0;
+      case P_SIBC_E: return nsibc > 0;
+      case P_SRC_E:
+      case P_SRC_H:
+        for (const auto &l : srcs)
+          if ((l.c <= EZ) == (part == P_SRC_E)) return true;
+        return false;
+      case P_TFSF_E:
+      case P_TFSF_H:
+        for (const auto &w : pws)
+          if (w.pv.use_aux || (part == P_TFSF_E ? w.total_e : w.total_h)) return true;
+        return false;
+      case P_GHOST_E: return ghost_e;
+      case P_MUR_H: return mvh.nitems > 0;
+      case P_SWEEP_H: return sw_h[0].ntiles || sw_h[1].ntiles;
+      case P_SIBC_H: return nsibc > 0 && ntgt > 0;
+      case P_GHOST_H: return ghost_h;
+      default: return false;
+    }
+  }
+
+  int launch_part(int part, int rel, uint64_t *count)
+  {
+    uint64_t launches = 0;
+    switch (part) {
+      case P_OBSERVE:
+        if (p.num_td || p.num_fd) {
+          int nt = (p.num_td + p.num_fd) * 6;
+          k_observe<T><<<blocks_for(nt, 128), 128, 0, s>>>(g, d_td_pts, p.num_td, d_fd_pts, p.num_fd, d_td, d_stage,
+                                                            d_step, rel, p.out_start, p.out_stop, kTB);
+          launches++;
+        }
+        break;
+      case P_BIN:
+        if (p.num_bin > 0) {
+          k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step,
+                                                                          rel, p.out_start, p.out_stop, kChunk);
+          launches++;
+        }
+        break;
+      // Mur reads the neighbours' pre-update E, so it precedes the sweeps;
+      // the PML and bulk sweeps touch disjoint E points.
+      case P_MUR_E:
+        if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
+        break;
+      case P_SWEEP_E:
+        if (int rc = launch_sweep_pair(true, &launches)) return rc;
+        break;
+      case P_DEBYE:
+        if (n_debye) {
+          k_debye<T><<<blocks_for(debye_total, 128), 128, 0, s>>>(g, d_debye, n_debye, debye_total, d_J, d_lastE,
+                                                                  d_dcoef);
+          launches++;
+        }
+        break;
+      case P_SIBC_E:
+        if (nsibc) {
+          k_sibc_e<T><<<blocks_for(sibc_faces, 128), 128, 0, s>>>(g, d_surfs, nsibc, d_models, d_q0, d_q1, d_q2,
+                                                                  d_adjA, d_adjB, d_zofs, d_zeta, d_old, d_etan,
+                                                                  sibc_faces);
+          launches++;
+        }
+        break;
+      case P_SRC_E:
+      case P_SRC_H:
+        for (auto &l : srcs)
+          if ((l.c <= EZ) == (part == P_SRC_E)) {
+            k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft,
+                                                                     (const T *)l.values, d_step, rel);
+            launches++;
+          }
+        break;
+      case P_TFSF_E:
+        for (auto &w : pws) {
+          if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, rel); launches++; }
+          if (w.total_e) {
+            k_tfsf_list<T><<<blocks_for(tfsf_threads(w.le), 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step,
+                                                                                rel, 1);
+            launches++;
+          }
+        }
+        break;
+      case P_GHOST_E:
+        if (ghost_e) {
+          k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 6), 128, 0, s>>>(g, gv, 1, 0);
+          launches++;
+        }
+        break;
+      case P_MUR_H:
+        if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
+        break;
+      case P_SWEEP_H:
+        if (int rc = launch_sweep_pair(false, &launches)) return rc;
+        break;
+      case P_SIBC_H:
+        if (nsibc && ntgt) {
+          k_sibc_h<T><<<blocks_for(ntgt, 128), 128, 0, s>>>(g, d_tgt_index, d_tgt_comp, d_tgt_start, ntgt, d_ops,
+                                                            d_etan);
+          launches++;
+        }
+        break;
+      case P_TFSF_H:
+        for (auto &w : pws) {
+          if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
+          if (w.total_h) {
+            k_tfsf_list<T><<<blocks_for(tfsf_threads(w.lh), 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step,
+                                                                                rel, 0);
+            launches++;
+          }
+        }
+        break;
+      case P_GHOST_H:
+        if (ghost_h) {
+          k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 12), 128, 0, s>>>(g, gv, 0, 0);
+          launches++;
+        }
+        break;
+      default: return set_err(VGPU_EINVAL, "no step part %d", part);
+    }
+    if (count) *count += launches;
+    return 0;
+  }
+
   int enqueue_step(int rel)
   {
     uint64_t launches = 0;
-    const dim3 blk(32, 8);
-    if (p.num_td || p.num_fd) {
-      int nt = (p.num_td + p.num_fd) * 6;
-      k_observe<T><<<blocks_for(nt, 128), 128, 0, s>>>(g, d_td_pts, p.num_td, d_fd_pts, p.num_fd, d_td, d_stage, d_step,
-                                                        rel, p.out_start, p.out_stop, kTB);
-      launches++;
-    }
-    if (p.num_bin > 0) {
-      k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step, rel,
-                                                                      p.out_start, p.out_stop, kChunk);
-      launches++;
-    }
-    // Mur reads the neighbours' pre-update E, so it precedes the sweeps; the
-    // PML and bulk sweeps touch disjoint E points.
-    if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
-    if (int rc = launch_sweep_pair(true, &launches)) return rc;
-    if (n_debye) {
-      k_debye<T><<<blocks_for(debye_total, 128), 128, 0, s>>>(g, d_debye, n_debye, debye_total, d_J, d_lastE, d_dcoef);
-      launches++;
-    }
-    if (nsibc) {
-      k_sibc_e<T><<<blocks_for(sibc_faces, 128), 128, 0, s>>>(g, d_surfs, nsibc, d_models, d_q0, d_q1, d_q2, d_adjA,
-                                                              d_adjB, d_zofs, d_zeta, d_old, d_etan, sibc_faces);
-      launches++;
-    }
-    for (auto &l : srcs)
-      if (l.c <= EZ) {
-        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, rel);
-        launches++;
-      }
-    for (auto &w : pws) {
-      if (w.pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(w.pv, d_step, rel); launches++; }
-      if (w.total_e) {
-        k_tfsf_list<T><<<blocks_for(tfsf_threads(w.le), 128), 128, 0, s>>>(g, w.pv, w.te, w.le, p.dt, d_step, rel, 1);
-        launches++;
-      }
-    }
-    if (ghost_e) {
-      k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 6), 128, 0, s>>>(g, gv, 1, 0);
-      launches++;
-    }
-    if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
-    if (int rc = launch_sweep_pair(false, &launches)) return rc;
-    if (nsibc && ntgt) {
-      k_sibc_h<T><<<blocks_for(ntgt, 128), 128, 0, s>>>(g, d_tgt_index, d_tgt_comp, d_tgt_start, ntgt, d_ops, d_etan);
-      launches++;
-    }
-    for (auto &l : srcs)
-      if (l.c > EZ) {
-        k_source<T><<<blocks_for(l.b.count(), 128), 128, 0, s>>>(g, l.b, l.c, l.kind, (T)l.soft, (const T *)l.values, d_step, rel);
-        launches++;
-      }
-    for (auto &w : pws) {
-      if (w.pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(w.pv); launches++; }
-      if (w.total_h) {
-        k_tfsf_list<T><<<blocks_for(tfsf_threads(w.lh), 128), 128, 0, s>>>(g, w.pv, w.th, w.lh, p.dt, d_step, rel, 0);
-        launches++;
-      }
-    }
-    if (ghost_h) {
-      k_ghost<T><<<dim3(blocks_for(ghost_threads, 128), 12), 128, 0, s>>>(g, gv, 0, 0);
-      launches++;
-    }
+    for (int part = 0; part < P_COUNT; part++)
+      if (int rc = launch_part(part, rel, &launches)) return rc;
     launches_per_step = launches;
     return 0;
   }
@@ -1526,15 +1613,46 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  int capture_graph()
+  // Graph q holds kGraphSteps >> q steps (16, 8, 4, 2, 1) and the counter's
+  // advance past them.  The 16-step graph is captured at creation, the
+  // shorter ones on first use: a block that does not start on a 16-step
+  // boundary (a run of any length, a service's partial block) is replayed
+  // from graphs too, largest first, instead of single kernel launches.
+  static constexpr int kNumGraphs = 5;
+
+  int capture_graph(int q = 0)
   {
-    cudaGraph_t gr;
+    cudaGraph_t gr = nullptr;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    enqueue_steps(kGraphSteps);
-    CK(cudaStreamEndCapture(s, &gr));
-    cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+    const int rc = enqueue_steps(kGraphSteps >> q);
+    const cudaError_t ee = cudaStreamEndCapture(s, &gr);
+    if (rc) {
+      if (ee == cudaSuccess && gr) cudaGraphDestroy(gr);
+      return rc;
+    }
+    if (ee != cudaSuccess) return set_err(VGPU_ECUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ee));
+    const cudaError_t e = cudaGraphInstantiate(&graphs[q], gr, 0);
     cudaGraphDestroy(gr);
-    if (e != cudaSuccess) return set_err(VGPU_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      graphs[q] = nullptr;
+      return set_err(VGPU_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    return 0;
+  }
+
+  // m steps as graph launches, largest graphs first.
+  int launch_graphs(uint64_t m)
+  {
+    for (int q = 0; q < kNumGraphs && m; q++) {
+      const uint64_t len = (uint64_t)(kGraphSteps >> q);
+      while (m >= len) {
+        if (!graphs[q])
+          if (int rc = capture_graph(q)) return rc;
+        CK(cudaGraphLaunch(graphs[q], s));
+        stats.kernel_launches += len * launches_per_step + 1;
+        m -= len;
+      }
+    }
     return 0;
   }
 
@@ -1545,16 +1663,18 @@ struct Engine : EngineBase {
     int nrows = (int)(r1 - r0);
     int nf = p.num_freq, npc = p.num_fd * 6;
     k_twiddle<<<blocks_for((int64_t)nrows * nf, 128), 128, 0, s>>>(d_omega, nf, p.dt, p.out_start, r0, nrows, d_tw);
-    dim3 blk(32, 8), grd((nf + 31) / 32, (npc + 7) / 8);
-    size_t shm = sizeof(double) * 8 * nrows;
-    k_dft_accumulate<<<grd, blk, shm, s>>>(d_stage, npc, nf, nrows, (int)(r0 % kTB), kTB, d_tw, d_re, d_im);
-    stats.kernel_launches += 2;
+    const int tiles = (npc + kDftTileM - 1) / kDftTileM;
+    for (int t0 = 0; t0 < tiles; t0 += 65535) {
+      const dim3 grd((nf + kDftTileF - 1) / kDftTileF, std::min(65535, tiles - t0));
+      k_dft_mma<<<grd, 128, 0, s>>>(d_stage, npc, nf, nrows, (int)(r0 % kTB), kTB, d_tw, d_re, d_im, t0 * kDftTileM);
+      stats.kernel_launches += 1;
+    }
+    stats.kernel_launches += 1;
     return 0;
   }
 
-  // Queue the next block of at most max_steps steps (four launches of the
-  // 16-step graph, or single steps up to the next 64-step boundary) on the
-  // engine's stream, with the block's DFT fold and binary-row copy; *queued
+  // Queue the next block of at most max_steps steps (up to the next 64-step
+  // boundary, replayed from the step graphs) on the engine's stream, with the block's DFT fold and binary-row copy; *queued
   // gets the count.
   int issue_block(uint64_t max_steps, uint64_t *queued)
   {
@@ -1570,12 +1690,7 @@ struct Engine : EngineBase {
     // they are overwritten.
     if (p.num_bin > 0)
       if (int rc = bin_deliver(q)) return rc;
-    if (m == (uint64_t)kChunk) {
-      for (int r = 0; r < kChunk / kGraphSteps; r++) CK(cudaGraphLaunch(graph, s));
-    } else {
-      if (int rc = enqueue_steps((int)m)) return rc;
-    }
-    stats.kernel_launches += m * launches_per_step + (m == (uint64_t)kChunk ? kChunk / kGraphSteps : 1);
+    if (int rc = launch_graphs(m)) return rc;
     step += m;
     // Output rows produced in this block.
     const uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
@@ -1585,7 +1700,19 @@ struct Engine : EngineBase {
     if (p.num_fd && hi >= lo) {
       if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
     }
+    if (step % kChunk == 0 || step == p.num_steps)
+      if (int rc = queue_energy()) return rc;
     *queued = m;
+    return 0;
+  }
+
+  // The stability check of the fields as they stand after the queued steps.
+  int queue_energy()
+  {
+    CK(cudaMemsetAsync(d_energy, 0, 2 * sizeof(double), s));
+    k_energy<T><<<4 * 148, 256, 0, s>>>(g, vol, d_energy);
+    stats.kernel_launches += 1;
+    energy_step = step;
     return 0;
   }
 
@@ -1594,6 +1721,16 @@ struct Engine : EngineBase {
   int finish_queued()
   {
     if (int rc = check_device_error()) return rc;
+    if (energy_step) {
+      double en[2] = { 0, 0 };
+      CK(cudaMemcpy(en, d_energy, sizeof en, cudaMemcpyDeviceToHost));
+      stats.energy_e = en[0];
+      stats.energy_h = en[1];
+      stats.energy_step = energy_step;
+      if (!std::isfinite(en[0]) || !std::isfinite(en[1]))
+        return set_err(VGPU_ENONFINITE, "the fields' FP64 sums of squares are not finite at step %llu",
+                       (unsigned long long)energy_step);
+    }
     if (p.num_bin > 0) {
       int a = 0, b = 1;
       if (bin_blk[1].pending && (!bin_blk[0].pending || bin_blk[1].row0 < bin_blk[0].row0)) a = 1, b = 0;
@@ -1644,7 +1781,15 @@ struct Engine : EngineBase {
     return issue_block(std::min<uint64_t>(max_steps, left), queued);
   }
 
-  int query() override { return cudaStreamQuery(s) == cudaSuccess ? 1 : 0; }
+  // 1: the queued work has finished; 0: still running; a device error
+  // (sticky or not) is reported, never read as "still running".
+  int query() override
+  {
+    const cudaError_t e = cudaStreamQuery(s);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return set_err(VGPU_ECUDA, "stream query: %s", cudaGetErrorString(e));
+  }
 
   int synchronize() override
   {
@@ -1714,19 +1859,53 @@ struct Engine : EngineBase {
     return 0;
   }
 
+  // The step part a VGPU_K_* id above the sweeps names (-1: none).
+  static int part_of(int kernel)
+  {
+    static const int map[] = { P_OBSERVE, P_BIN, P_MUR_E, P_DEBYE, P_SIBC_E, P_SRC_E, P_TFSF_E, P_GHOST_E,
+                               P_MUR_H, P_SIBC_H, P_SRC_H, P_TFSF_H, P_GHOST_H };
+    const int q = kernel - VGPU_K_OBSERVE;
+    return q >= 0 && q < (int)(sizeof map / sizeof map[0]) ? map[q] : -1;
+  }
+
+  // One launch of a timed kernel: a sweep, a step part or a 64-row DFT fold.
+  int launch_timed(int kernel)
+  {
+    if (kernel >= 0 && kernel <= 3) return launch_one(kernel);
+    if (kernel == VGPU_K_DFT_BLOCK) {
+      const uint64_t st = stats.kernel_launches;
+      const int rc = dft_rows(0, kTB);
+      stats.kernel_launches = st;
+      return rc;
+    }
+    return launch_part(part_of(kernel), 0, nullptr);
+  }
+
   int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override
   {
-    uint64_t bulk_pts = 0, pml_pts = 0;
-    if (int rc = sweep_points(kernel, &bulk_pts, &pml_pts)) return rc;
-    const uint64_t pts = bulk_pts + pml_pts;
+    uint64_t pts = 0;
+    if (kernel >= 0 && kernel <= 3) {
+      uint64_t bulk_pts = 0, pml_pts = 0;
+      if (int rc = sweep_points(kernel, &bulk_pts, &pml_pts)) return rc;
+      pts = bulk_pts + pml_pts;
+      const bool es = kernel == VGPU_K_BULK_E || kernel == VGPU_K_PML_E;
+      if (!(es ? sw_e : sw_h)[(kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) ? 0 : 1].ntiles)
+        return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
+    } else if (kernel == VGPU_K_DFT_BLOCK) {
+      if (!p.num_fd) return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
+    } else {
+      const int part = part_of(kernel);
+      if (part < 0) return set_err(VGPU_EINVAL, "kernel %d is not a step kernel", kernel);
+      if (!part_present(part)) return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
+    }
     for (int q = 0; q < warmup; q++)
-      if (int rc = launch_one(kernel)) return rc;
+      if (int rc = launch_timed(kernel)) return rc;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, s));
     for (int q = 0; q < iters; q++)
-      if (int rc = launch_one(kernel)) return rc;
+      if (int rc = launch_timed(kernel)) return rc;
     CK(cudaEventRecord(e1, s));
     CK(cudaEventSynchronize(e1));
     CK(cudaGetLastError());
@@ -1984,23 +2163,35 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
     if (int rc = on_dev(engines[i])->check_steps(steps[i])) return rc;
   }
   std::vector<uint64_t> left(steps, steps + n);
-  for (bool any = true; any;) {
+  // On a queueing error nothing more is queued, but every engine's queued
+  // blocks are still waited for: the caller gets control back only when no
+  // engine of the batch is stepping.  The first error is returned.
+  int rc = 0;
+  std::string msg;
+  for (bool any = true; any && !rc;) {
     any = false;
-    for (int32_t i = 0; i < n; i++) {
+    for (int32_t i = 0; i < n && !rc; i++) {
       if (!left[i]) continue;
       uint64_t m = 0;
-      if (int rc = on_dev(engines[i])->enqueue(left[i], &m)) return rc;
-      // An engine listed twice can reach its last step before its count.
-      if (!m) return set_err(VGPU_EINVAL, "engine %d in batch reached its last step", (int)i);
+      if (int r = on_dev(engines[i])->enqueue(left[i], &m)) {
+        rc = r;
+      } else if (!m) {
+        // An engine listed twice can reach its last step before its count.
+        rc = set_err(VGPU_EINVAL, "engine %d in batch reached its last step", (int)i);
+      }
+      if (rc) msg = g_err;
       left[i] -= m;
       any = any || left[i] > 0;
     }
   }
-  int rc = 0;
   for (int32_t i = 0; i < n; i++) {
     int r = on_dev(engines[i])->synchronize();
-    if (r && !rc) rc = r;
+    if (r && !rc) {
+      rc = r;
+      msg = g_err;
+    }
   }
+  if (rc) set_err(rc, "%s", msg.c_str());
   return rc;
 }
 
@@ -2032,6 +2223,13 @@ extern "C" int vgpu_get_stats(const vgpu_engine *e, vgpu_stats *st)
   return 0;
 }
 
+extern "C" int vgpu_set_sweep_wait_limit(int64_t polls)
+{
+  const uint32_t v = polls < 0 ? kSpinLimit : (uint32_t)std::min<int64_t>(polls, kSpinLimit);
+  CK(cudaMemcpyToSymbol(g_full_wait_polls, &v, sizeof v));
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free running DFT for callers that cannot allocate device
 // memory.  The twiddle table lives in a file-scope device array; every GPU
@@ -2050,6 +2248,9 @@ extern "C" int vgpu_dft_accumulate_static(const double *samples, int32_t num_ser
   if (num_series <= 0 || num_rows <= 0 || num_freq <= 0) return set_err(VGPU_EINVAL, "sizes must be positive");
   if (num_rows > VGPU_STATIC_DFT_MAX_ROWS)
     return set_err(VGPU_EINVAL, "num_rows %d exceeds the maximum of %d rows per call", num_rows, VGPU_STATIC_DFT_MAX_ROWS);
+  if (num_series > VGPU_STATIC_DFT_MAX_SERIES)
+    return set_err(VGPU_EINVAL, "num_series %d exceeds the maximum of %d series per call", num_series,
+                   VGPU_STATIC_DFT_MAX_SERIES);
   if ((int64_t)num_rows * num_freq > VGPU_STATIC_DFT_MAX_ENTRIES)
     return set_err(VGPU_EINVAL, "num_rows * num_freq = %lld exceeds the static twiddle table of %d entries",
                    (long long)num_rows * num_freq, VGPU_STATIC_DFT_MAX_ENTRIES);

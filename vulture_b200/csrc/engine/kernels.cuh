@@ -401,6 +401,89 @@ __global__ void k_dft_accumulate(const double *stage, int npc, int nf, int nrows
   im[(int64_t)pc * nf + f] = ai;
 }
 
+// The same fold as a GEMM on the FP64 tensor cores (the tcgen05 MMA kinds
+// have no f64 form; the FP64 MMA is mma.sync m8n8k4).  For a block of rows
+// r = 0..nrows-1 and a tile of 64 point-components x 32 frequencies:
+//   re[pc][f] += sum_r v[r][pc] * cos(w_f t_r)
+//   im[pc][f] += sum_r v[r][pc] * (-sin(w_f t_r))
+// i.e. D[pc][2f + {0,1}] = A[pc][r] x B[r][2f + {0,1}] with the twiddle
+// columns interleaved (cos, -sin), so each thread's two accumulators of an
+// 8x8 tile are the re and im of one (pc, f).  The rows' sum is formed in
+// FP64 FMAs and then added to the running sums (src/observer.c:857-899 adds
+// row by row; the two orders agree to rounding).  Rows are taken 32 at a
+// time through shared memory; rows past nrows read as zero.
+constexpr int kDftTileM = 64;          // point-components per block (4 warps x 16)
+constexpr int kDftTileF = 32;          // frequencies per block (64 twiddle columns)
+constexpr int kDftTileK = 32;          // rows per shared-memory pass
+constexpr int kDftPad = 4;             // row padding: conflict-free fragment loads
+
+__device__ __forceinline__ void mma_f64_m8n8k4(double (&d)[2], double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) k_dft_mma(const double *__restrict__ stage, int npc, int nf, int nrows,
+                                                 int row_offset, int tblock, const double2 *__restrict__ tw,
+                                                 double *__restrict__ re, double *__restrict__ im, int pc0)
+{
+  __shared__ double As[kDftTileK][kDftTileM + kDftPad];        // [row][pc]
+  __shared__ double Bs[kDftTileK][2 * kDftTileF + kDftPad];    // [row][2f + (cos, -sin)]
+  // Launches cover at most 65535 tiles of point-components; pc0 is the
+  // first one of this launch.
+  const int m0 = pc0 + blockIdx.y * kDftTileM, f0 = blockIdx.x * kDftTileF;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, t = lane & 3;   // fragment row group and column in group
+  double acc[2][8][2];
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+    for (int ni = 0; ni < 8; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+  for (int r0 = 0; r0 < nrows; r0 += kDftTileK) {
+    const int kr = min(kDftTileK, nrows - r0);
+    for (int q = tid; q < kDftTileK * kDftTileM; q += 128) {
+      const int r = q / kDftTileM, c = q % kDftTileM, pc = m0 + c;
+      As[r][c] = (r < kr && pc < npc) ? stage[(int64_t)((row_offset + r0 + r) % tblock) * npc + pc] : 0.0;
+    }
+    for (int q = tid; q < kDftTileK * kDftTileF; q += 128) {
+      const int r = q / kDftTileF, c = q % kDftTileF, f = f0 + c;
+      const double2 w = (r < kr && f < nf) ? tw[(int64_t)(r0 + r) * nf + f] : make_double2(0.0, 0.0);
+      Bs[r][2 * c] = w.x;
+      Bs[r][2 * c + 1] = -w.y;
+    }
+    __syncthreads();
+    const int kp = (kr + 3) & ~3;
+    for (int k = 0; k < kp; k += 4) {
+      double a[2], b[8];
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++) a[mi] = As[k + t][16 * warp + 8 * mi + g];
+#pragma unroll
+      for (int ni = 0; ni < 8; ni++) b[ni] = Bs[k + t][8 * ni + g];
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 8; ni++) mma_f64_m8n8k4(acc[mi][ni], a[mi], b[ni]);
+    }
+    __syncthreads();
+  }
+  // acc[mi][ni][j] = D[16 warp + 8 mi + g][8 ni + 2 t + j]: column pair
+  // (8 ni + 2 t, +1) is frequency 4 ni + t of the tile, (re, im).
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++) {
+    const int pc = m0 + 16 * warp + 8 * mi + g;
+    if (pc >= npc) continue;
+#pragma unroll
+    for (int ni = 0; ni < 8; ni++) {
+      const int f = f0 + 4 * ni + t;
+      if (f >= nf) continue;
+      const int64_t x = (int64_t)pc * nf + f;
+      re[x] = re[x] + acc[mi][ni][0];
+      im[x] = im[x] + acc[mi][ni][1];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Waveforms on the device (src/waveform.c:412-638), used by the analytic
 // plane-wave incident field.  Evaluated in double.
@@ -801,6 +884,56 @@ __global__ void k_finite(Grid<T> g, int64_t vol_padded, int *flag)
   for (; t < vol_padded; t += stride)
     for (int c = 0; c < 6; c++)
       if (!isfinite((double)g.F[c][t])) { atomicExch(flag, 1); return; }
+}
+
+// Stability check (FP64): sums of squares of the three E and of the three H
+// components over every stored point, added into out[0] and out[1].  Not the
+// physical energy (no permittivity, permeability or cell-volume weights) but
+// a norm of the fields that grows without bound once the update is unstable
+// and turns non-finite with any field value.  The reference's only guard is
+// the Courant-number check before the loop (src/simulation.c:64-84).  One
+// atomic add per block and quantity.
+template <typename T>
+__global__ void k_energy(Grid<T> g, int64_t vol_padded, double *out)
+{
+  double e = 0.0, h = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < vol_padded; t += stride) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double v = (double)g.F[c][t];
+      e = e + v * v;
+    }
+#pragma unroll
+    for (int c = 3; c < 6; c++) {
+      const double v = (double)g.F[c][t];
+      h = h + v * v;
+    }
+  }
+  __shared__ double se[32], sh[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, o);
+    h += __shfl_down_sync(0xffffffffu, h, o);
+  }
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  if (l == 0) {
+    se[w] = e;
+    sh[w] = h;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (int)(blockDim.x / 32);
+    e = l < nw ? se[l] : 0.0;
+    h = l < nw ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      e += __shfl_down_sync(0xffffffffu, e, o);
+      h += __shfl_down_sync(0xffffffffu, h, o);
+    }
+    if (l == 0) {
+      atomicAdd(&out[0], e);
+      atomicAdd(&out[1], h);
+    }
+  }
 }
 
 }  // namespace vgpu_dev

@@ -87,12 +87,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t polls = kSpinLimit)
 {
-  for (uint32_t it = 0; it < kSpinLimit; ++it)
+  for (uint32_t it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+
+// Polls a compute warp makes on a stage's data barrier before it gives up.
+// kSpinLimit unless a test lowers it (vgpu_set_sweep_wait_limit) to make the
+// wait run out; the producer's waits always keep kSpinLimit, so a block
+// whose compute warps left still waits for every load it issued.
+__device__ uint32_t g_full_wait_polls = kSpinLimit;
 
 // 3-D tiled TMA load of one box into shared memory, completing on `bar`.
 // No multicast: the source is always this GPU's own memory.
@@ -312,6 +318,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
   }
 
   // ---- compute warps ----
+  const uint32_t full_polls = *(volatile uint32_t *)&g_full_wait_polls;
   const int kl = tid % KW, jl = tid / KW;
   T *__restrict__ F0 = g.F[ESWEEP ? EX : HX];
   T *__restrict__ F1 = g.F[ESWEEP ? EY : HY];
@@ -323,7 +330,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
     if ((int)(blockIdx.x + m * gridDim.x) >= ntiles) return;
     // Stage 0 of the tile, with its header.
     uint32_t slot = gs % S;
-    bool ok = mbar_wait(&full[slot], (gs / S) & 1);
+    bool ok = mbar_wait(&full[slot], (gs / S) & 1, full_polls);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicCAS(err, 0, 1);
       return;
@@ -363,7 +370,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
 
     for (int p = 0; p < n; p++) {
       slot = gs % S;
-      ok = mbar_wait(&full[slot], (gs / S) & 1);
+      ok = mbar_wait(&full[slot], (gs / S) & 1, full_polls);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) atomicCAS(err, 0, 1);
         return;

@@ -183,25 +183,29 @@ class Server:
                 self.peak_active = max(self.peak_active, len(active))
                 still = []
                 for r, mesh, run, path in active:
-                    if not run.done():
+                    try:
+                        # A device error on the solve's stream ends the solve
+                        # here, instead of reading as work still in flight.
+                        finished = run.done()
+                        if finished and run.step >= mesh.num_steps:
+                            run.synchronize()
+                            if keep_results:
+                                r.td = run.td()
+                                r.dft = run.dft()
+                    except N.NativeError as exc:   # a device-side failure of this solve
+                        self._fail(r, exc, t0)
+                        run.close()
+                        mesh.close()
+                        os.unlink(path)
+                        used -= r.estimate
+                        progressed = True
+                        continue
+                    if not finished:
                         still.append((r, mesh, run, path))
                         continue
                     if run.step >= mesh.num_steps:
-                        try:
-                            run.synchronize()
-                        except N.NativeError as exc:   # a device-side failure of this solve
-                            self._fail(r, exc, t0)
-                            run.close()
-                            mesh.close()
-                            os.unlink(path)
-                            used -= r.estimate
-                            progressed = True
-                            continue
                         r.completed = time.perf_counter() - t0
                         r.cell_updates = mesh.num_cells * mesh.num_steps
-                        if keep_results:
-                            r.td = run.td()
-                            r.dft = run.dft()
                         run.close()
                         mesh.close()
                         os.unlink(path)
@@ -286,26 +290,29 @@ def solve_batch(meshes, precision: str = "fp32", budget_bytes: int | None = None
     result = [None] * len(meshes)
     for wave in waves:
         runs = []
+        handed_over = False
         try:
             for q in wave:
                 runs.append(GpuRun(meshes[q], precision))
-        except BaseException:
-            for r in runs:
-                r.close()
-            raise
-        started = time.perf_counter() - t0
-        run_batch(runs)
-        finished = time.perf_counter() - t0
-        for q, r in zip(wave, runs):
-            r.batch_started, r.batch_finished = started, finished
+            started = time.perf_counter() - t0
+            run_batch(runs)
+            finished = time.perf_counter() - t0
+            for q, r in zip(wave, runs):
+                r.batch_started, r.batch_finished = started, finished
             if budget_bytes is None:
-                result[q] = r
-                continue
-            try:
-                if on_done is not None:
+                for q, r in zip(wave, runs):
+                    result[q] = r
+                handed_over = True
+            elif on_done is not None:
+                for q, r in zip(wave, runs):
                     on_done(q, r)
-            finally:
-                r.close()
+        finally:
+            # Every engine of a budgeted wave is freed before the next wave,
+            # and on any error (creation, stepping, a failing callback) no
+            # engine of the wave outlives the call.
+            if not handed_over:
+                for r in runs:
+                    r.close()
     return result if budget_bytes is None else None
 
 

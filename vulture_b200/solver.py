@@ -189,8 +189,12 @@ class GpuRun:
         return q.value
 
     def done(self) -> bool:
-        """True when the queued steps have finished on the device."""
-        return N.lib().vgpu_query(self._e) == 1
+        """True when the queued steps have finished on the device; raises
+        NativeError when the engine's stream reports a device error."""
+        rc = N.lib().vgpu_query(self._e)
+        if rc < 0:
+            N.check_gpu(rc)
+        return rc == 1
 
     def synchronize(self):
         N.check_gpu(N.lib().vgpu_synchronize(self._e))
