@@ -323,6 +323,29 @@ def kernel_split(g, steps_per_block: int = 64):
                     "64-step block divided by 64; the sum omits the launch gaps of a real step"}
 
 
+def full_run_legs(args, m, prec, e2e_run, dist, world, n_out, nt_full):
+    """The workload's whole run (its own 4000 steps) end to end through the C
+    ABI, and the same run in plain FP64: the FP64 path's throughput and the
+    FP32 error per result against it."""
+    full = e2e_run(prec, nt_full)
+    full_wall = max_over_ranks(full["wall_s"], dist)
+    e2e_full = {"steps": nt_full, "value": world * n_out * nt_full / full_wall / 1e6, "unit": "Mcell-updates/s",
+                "wall_s": full_wall, "create_s": full["create_s"], "step_s": full["step_s"],
+                "read_s": full["read_s"], "h2d_bytes": full["h2d"], "d2h_bytes": full["d2h"],
+                "device_mcell_per_s": n_out * nt_full / (full["run_ms"] * 1e-3) / 1e6,
+                "what": "the workload's whole run through the C ABI: create + all steps + observer read-back"}
+    fp64 = None
+    fp32_error = None
+    if prec == "fp32" and not args.no_fp64:
+        f64 = e2e_run("fp64", nt_full)
+        fp64 = n_out * nt_full / (f64["run_ms"] * 1e-3) / 1e6
+        names = [m.observer_name(True, q) for q in range(m.num_fd)]
+        fp32_error = error_report(full["td"], full["re"], full["im"], f64["td"], f64["re"], f64["im"], nt_full,
+                                  names)
+
+    return e2e_full, fp64, fp32_error
+
+
 def run_gpu_arm(args):
     import numpy as np
     import torch
@@ -419,22 +442,11 @@ def run_gpu_arm(args):
     # run in plain FP64: the FP32 error per result against it, and the FP64
     # path's throughput.
     nt_full = m.num_steps
-    full = e2e_run(prec, nt_full)
-    full_wall = max_over_ranks(full["wall_s"], dist)
-    e2e_full = {"steps": nt_full, "value": world * n_out * nt_full / full_wall / 1e6, "unit": "Mcell-updates/s",
-                "wall_s": full_wall, "create_s": full["create_s"], "step_s": full["step_s"],
-                "read_s": full["read_s"], "h2d_bytes": full["h2d"], "d2h_bytes": full["d2h"],
-                "device_mcell_per_s": n_out * nt_full / (full["run_ms"] * 1e-3) / 1e6,
-                "what": "the workload's whole run through the C ABI: create + all steps + observer read-back"}
-    fp64 = None
-    fp32_error = None
-    if prec == "fp32" and not args.no_fp64:
-        f64 = e2e_run("fp64", nt_full)
-        fp64 = n_out * nt_full / (f64["run_ms"] * 1e-3) / 1e6
-        names = [m.observer_name(True, q) for q in range(m.num_fd)]
-        fp32_error = error_report(full["td"], full["re"], full["im"], f64["td"], f64["re"], f64["im"], nt_full,
-                                  names)
+    e2e_full = fp64 = fp32_error = None
+    if not args.no_full_run:
+        e2e_full, fp64, fp32_error = full_run_legs(args, m, prec, e2e_run, dist, world, n_out, nt_full)
 
+    sub = {}
     sub = {}
     if not args.no_enclosure:
         sub["enclosure"] = enclosure_workload(args, dist)
@@ -807,6 +819,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--workload", default="graded", choices=["graded", "enclosure", "batch", "serve"])
     ap.add_argument("--no-enclosure", action="store_true", help="graded workload without the enclosure sub-object")
+    ap.add_argument("--no-full-run", action="store_true",
+                    help="graded workload without the whole-run e2e and FP32-error legs")
     ap.add_argument("--no-batch", action="store_true", help="graded workload without the batch sub-object")
     ap.add_argument("--no-serve", action="store_true", help="graded workload without the serve sub-object")
     ap.add_argument("--batch-count", type=int, default=256)

@@ -251,6 +251,12 @@ typedef struct {
    * VGPU_ENONFINITE when it is not finite. */
   double energy_e, energy_h;
   uint64_t energy_step;
+  /* Side launches the engine merged for this problem: bit 0, the Debye
+   * update and the plane wave's E corrections run as one kernel; bit 1, the
+   * plane wave's H corrections and the next step's observer samples do.  Set
+   * only where the merged parts touch disjoint points. */
+  uint32_t merged_parts;
+  uint32_t reserved;
 } vgpu_stats;
 
 /* Create an engine on the current CUDA device (cuda:0 unless the caller set
@@ -347,8 +353,11 @@ enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 
 /* The other parts of a time step, in their order within the step
  * (src/simulation.c:156-222), and the DFT fold of one 64-step block
  * (src/observer.c:857-899), for vgpu_time_kernel.  Each part is the launch
- * (or launches: one per source or plane wave) of that update in the step;
- * timing a part the problem does not have is an error. */
+ * (or launches: one per source or plane wave) of that update as the step
+ * makes it: where vgpu_stats.merged_parts shows a merge, VGPU_K_DEBYE also
+ * applies the E corrections and VGPU_K_TFSF_H also takes the next step's
+ * samples, and VGPU_K_OBSERVE (or VGPU_K_TFSF_E without an auxiliary grid)
+ * launches nothing.  Timing a part with no launch is an error. */
 enum {
   VGPU_K_OBSERVE = 4, VGPU_K_BIN_OBSERVE = 5, VGPU_K_MUR_E = 6, VGPU_K_DEBYE = 7, VGPU_K_SIBC_E = 8,
   VGPU_K_SOURCES_E = 9, VGPU_K_TFSF_E = 10, VGPU_K_GHOST_E = 11, VGPU_K_MUR_H = 12, VGPU_K_SIBC_H = 13,

@@ -108,6 +108,31 @@ def many_media_mesh(nmedia=300, seed=5):
     return "\n".join(out) + "\n"
 
 
+def debye_tfsf_cubic_mesh(nt=200):
+    """A cubic grid (so the plane wave uses the 1-D auxiliary grid and every
+    value is bit-exact) with a Debye block and a TFSF plane wave inside a
+    UPML box, and observers off the Huygens faces: the engine merges the
+    Debye update with the E corrections, and the H corrections with the next
+    step's samples, into single launches (vgpu_stats.merged_parts = 3)."""
+    return "\n".join([
+        "VM 1.0.0", "CE Debye block and plane wave on a cubic grid", "DM 40 36 32", "GS",
+        "BT XLO PML 6", "BT XHI PML 6", "BT YLO PML 6", "BT YHI PML 6", "BT ZLO PML 6", "BT ZHI PML 6",
+        "MT deb DEBYE 2.0 0.0 1.0 1.000000e+10 -1.000000e+10", "MB 12 24 10 20 11 19 deb",
+        "WF wf1 GAUSSIAN_PULSE 1.0",
+        "PW 4 36 4 32 4 28 pw1 wf1 0.0 0.0 0.0 111111",
+        "OP 20 20 18 18 15 15 op1 TDOM_ASCII", "OP 14 14 12 12 13 13 op2 TDOM_ASCII",
+        "OP 25 25 22 22 17 17 op3 FDOM_ASCII", "OP 2 2 2 2 2 2 op4 TDOM_ASCII",
+        "GE", f"NT {nt}", "MS 0.005", "EN"]) + "\n"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_merged_side_launches_equal_oracle(precision):
+    m, g, c = solve_both(stage_text(debye_tfsf_cubic_mesh()), precision)
+    assert g.stats().merged_parts == 3
+    assert np.abs(c.td()).max() > 0
+    assert_same(m, g, c, dft_tol=1e-12 if precision == "fp64" else 1e-10)
+
+
 def synthetic():
     rng = random.Random(11)
     return {

@@ -27,7 +27,8 @@ VGPU_ECANCELLED = -7
 class VgpuStats(C.Structure):
     _fields_ = [("run_ms", C.c_double), ("steps", C.c_uint64), ("kernel_launches", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64), ("energy_e", C.c_double),
-                ("energy_h", C.c_double), ("energy_step", C.c_uint64)]
+                ("energy_h", C.c_double), ("energy_step", C.c_uint64),
+                ("merged_parts", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 # void sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows)

@@ -96,11 +96,18 @@ def build_reference() -> bool:
     ref = Path(os.environ.get("VULTURE_REF", str(ROOT.parent / "reference")))
     if not (ref / "src").is_dir():
         return False
-    want = ROOT / "oracle" / "_ref" / "vulture_oracle_f64_dump"
-    if want.exists():
+    out = ROOT / "oracle" / "_ref"
+    env = dict(os.environ, VULTURE_REF=str(ref))
+    if not (out / "vulture_oracle_f64_dump").exists():
+        subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh")], check=True, capture_output=True, env=env)
         return True
-    subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh")], check=True, capture_output=True,
-                   env=dict(os.environ, VULTURE_REF=str(ref)))
+    # The propagate() replacements compile against include/vgpu.h and the
+    # oracle: rebuild them when those change.
+    deps = [ROOT / "include" / "vgpu.h", ORACLE_SRC, *sorted((ROOT / "oracle" / "propagate_gpu").glob("*.c"))]
+    for name in ("vulture_ref_oracle_shim", "vulture_ref_gpu"):
+        if _stale(out / name, deps):
+            subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh"), name], check=True, capture_output=True,
+                           env=env)
     return True
 
 

@@ -47,7 +47,11 @@ extern "C" const char *vgpu_last_error(void) { return g_err; }
   } while (0)
 
 static const int kChunk = 64;      // steps per block and per DFT block
-static const int kTB = kChunk;     // DFT staging rows
+static const int kTwRows = kChunk; // twiddle rows of one DFT fold (one block)
+// DFT staging rows: two blocks' worth, so that the sample of a block's first
+// step, taken at the end of the previous block (merged side launch), never
+// lands on a row that block's fold has yet to read.
+static const int kStageRows = 2 * kChunk;
 static const int kGraphSteps = 16; // steps of the longest step graph; a full block replays it kChunk / kGraphSteps times
 
 // The device step counter moves once per block of steps; kernels inside
@@ -424,6 +428,11 @@ struct Engine : EngineBase {
   cudaStream_t ss = nullptr;
   // fused sweeps
   CoefIndex cie{}, cih{};
+  // Merged side launches (k_side), decided at set-up by plan_side_merges.
+  bool merge_e = false;      // the Debye cells and the plane wave's E corrections in one launch
+  bool merge_obs = false;    // the plane wave's H corrections and the next step's samples in one launch
+  bool need_sample = true;   // merge_obs: the current step's samples are still to be taken
+  SideLaunch<T> side_e{}, side_h{};
   // step graphs (capture_graph)
   cudaGraphExec_t graphs[5] = {};
   uint64_t launches_per_step = 0;
@@ -588,6 +597,7 @@ struct Engine : EngineBase {
     if (int rc = setup_observers()) return rc;
     pc.mark("observers");
     if (int rc = setup_sweeps()) return rc;
+    plan_side_merges();
     CK(cudaStreamSynchronize(ss));
     CK(cudaGetLastError());
     pc.mark("sweeps");
@@ -1367,6 +1377,10 @@ struct Engine : EngineBase {
     ghost_threads = maxp;
   }
 
+  // The last step sampled: the output window's end, or the problem's last
+  // step if the window runs past it (samples beyond it have no buffer row).
+  uint64_t out_last() const { return p.num_steps ? std::min<uint64_t>(p.out_stop, p.num_steps - 1) : 0; }
+
   int setup_observers()
   {
     if (p.num_steps > 0 && p.out_start < p.num_steps)
@@ -1375,8 +1389,8 @@ struct Engine : EngineBase {
       return VGPU_ENOMEM;
     if (mem.alloc(&d_td, (size_t)nout * p.num_td * 6)) return VGPU_ENOMEM;
     size_t npc = (size_t)p.num_fd * 6;
-    if (mem.alloc(&d_stage, npc * kTB) || mem.alloc(&d_re, npc * p.num_freq) || mem.alloc(&d_im, npc * p.num_freq) ||
-        mem.alloc(&d_tw, (size_t)kTB * p.num_freq))
+    if (mem.alloc(&d_stage, npc * kStageRows) || mem.alloc(&d_re, npc * p.num_freq) ||
+        mem.alloc(&d_im, npc * p.num_freq) || mem.alloc(&d_tw, (size_t)kTwRows * p.num_freq))
       return VGPU_ENOMEM;
     CK(cudaMemsetAsync(d_re, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1), ss));
     CK(cudaMemsetAsync(d_im, 0, sizeof(double) * (npc * p.num_freq ? npc * p.num_freq : 1), ss));
@@ -1501,14 +1515,14 @@ struct Engine : EngineBase {
         if (p.num_td || p.num_fd) {
           int nt = (p.num_td + p.num_fd) * 6;
           k_observe<T><<<blocks_for(nt, 128), 128, 0, s>>>(g, d_td_pts, p.num_td, d_fd_pts, p.num_fd, d_td, d_stage,
-                                                            d_step, rel, p.out_start, p.out_stop, kTB);
+                                                            d_step, rel, p.out_start, out_last(), kStageRows);
           launches++;
         }
         break;
       case P_BIN:
         if (p.num_bin > 0) {
           k_bin_observe<T><<<blocks_for(p.num_bin * 6, 128), 128, 0, s>>>(g, d_bin_pts, p.num_bin, d_bin, d_step,
-                                                                          rel, p.out_start, p.out_stop, kChunk);
+                                                                          rel, p.out_start, out_last(), kChunk);
           launches++;
         }
         break;
@@ -1595,11 +1609,98 @@ struct Engine : EngineBase {
     return 0;
   }
 
+  // Side launches that may share one kernel: the Debye update and the plane
+  // wave's E corrections follow the E sweep with nothing between them when
+  // there are no SIBC surfaces or E sources, and the plane wave's H
+  // corrections end the step when there is no ghost layer.  They share a
+  // launch only if they touch disjoint points -- no Debye cell of a component
+  // is a corrected point of it; no observer point is a corrected H point --
+  // so that their order does not matter.  Observer samples taken with the H
+  // corrections are those of the next step (src/observer.c:622-650 samples
+  // at the top of a step, i.e. the fields as the previous step left them).
+  void plan_side_merges()
+  {
+    bool e_src = false;
+    for (const auto &l : srcs) e_src = e_src || l.c <= EZ;
+    if (pws.size() == 1 && n_debye && pws[0].total_e && !nsibc && !e_src) {
+      bool disjoint = true;
+      for (int b = 0; b < p.num_debye && disjoint; b++)
+        for (int c = 0; c < 3 && disjoint; c++)
+          for (int q = 0; q < pws[0].te.n && disjoint; q++)
+            if (pws[0].te.it[q].c == c && boxes_meet(box_from(p.debye[b].flim[c]), pws[0].te.it[q].b)) disjoint = false;
+      merge_e = disjoint;
+    }
+    if (pws.size() == 1 && (p.num_td || p.num_fd) && p.num_bin <= 0 && pws[0].total_h && !ghost_h) {
+      bool disjoint = true;
+      for (int q = 0; q < pws[0].th.n && disjoint; q++) {
+        const Box &b = pws[0].th.it[q].b;
+        for (int t = 0; t < p.num_td && disjoint; t++)
+          if (b.contains(p.td_points[3 * t], p.td_points[3 * t + 1], p.td_points[3 * t + 2])) disjoint = false;
+        for (int t = 0; t < p.num_fd && disjoint; t++)
+          if (b.contains(p.fd_points[3 * t], p.fd_points[3 * t + 1], p.fd_points[3 * t + 2])) disjoint = false;
+      }
+      merge_obs = disjoint;
+    }
+    if (merge_e) {
+      SideLaunch<T> &L = side_e;
+      L.nb_debye = (int)blocks_for(debye_total, 128);
+      L.nb_tfsf = (int)blocks_for(tfsf_threads(pws[0].le), 128);
+      L.debye = d_debye; L.n_debye = n_debye; L.debye_total = debye_total;
+      L.J = d_J; L.lastE = d_lastE; L.dcoef = d_dcoef;
+      L.pw = pws[0].pv; L.tv = pws[0].te; L.tl = pws[0].le; L.dt = p.dt; L.efield = 1;
+    }
+    if (merge_obs) {
+      SideLaunch<T> &L = side_h;
+      L.nb_tfsf = (int)blocks_for(tfsf_threads(pws[0].lh), 128);
+      L.nb_obs = (int)blocks_for((int64_t)(p.num_td + p.num_fd) * 6, 128);
+      L.pw = pws[0].pv; L.tv = pws[0].th; L.tl = pws[0].lh; L.dt = p.dt; L.efield = 0;
+      L.td_pts = d_td_pts; L.num_td = p.num_td; L.fd_pts = d_fd_pts; L.num_fd = p.num_fd;
+      L.td_buf = d_td; L.fd_stage = d_stage; L.out_start = p.out_start; L.out_stop = out_last();
+      L.tblock = kStageRows;
+    }
+    stats.merged_parts = (merge_e ? 1u : 0u) | (merge_obs ? 2u : 0u);
+  }
+
+  // Whether the step launches anything for a part, merges included.
+  bool step_part_present(int part) const
+  {
+    if (merge_obs && part == P_OBSERVE) return false;
+    if (merge_e && part == P_TFSF_E) return pws[0].pv.use_aux != 0;
+    return part_present(part);
+  }
+
+  // One part as the step launches it: with merge_e the Debye part is the
+  // merged launch (after the auxiliary grid's E update, which the
+  // corrections read) and the TFSF E part is empty; with merge_obs the
+  // observer part is empty (the previous step's last launch took the
+  // samples) and the TFSF H part is the merged launch.
+  int launch_step_part(int part, int rel, uint64_t *count)
+  {
+    uint64_t launches = 0;
+    if (merge_e && (part == P_DEBYE || part == P_TFSF_E)) {
+      if (part == P_DEBYE) {
+        if (pws[0].pv.use_aux) { k_aux_e<T><<<1, 256, 0, s>>>(pws[0].pv, d_step, rel); launches++; }
+        k_side<T><<<side_e.nb_debye + side_e.nb_tfsf, 128, 0, s>>>(g, side_e, d_step, rel);
+        launches++;
+      }
+    } else if (merge_obs && (part == P_OBSERVE || part == P_TFSF_H)) {
+      if (part == P_TFSF_H) {
+        if (pws[0].pv.use_aux) { k_aux_h<T><<<1, 256, 0, s>>>(pws[0].pv); launches++; }
+        k_side<T><<<side_h.nb_tfsf + side_h.nb_obs, 128, 0, s>>>(g, side_h, d_step, rel);
+        launches++;
+      }
+    } else {
+      return launch_part(part, rel, count);
+    }
+    if (count) *count += launches;
+    return 0;
+  }
+
   int enqueue_step(int rel)
   {
     uint64_t launches = 0;
     for (int part = 0; part < P_COUNT; part++)
-      if (int rc = launch_part(part, rel, &launches)) return rc;
+      if (int rc = launch_step_part(part, rel, &launches)) return rc;
     launches_per_step = launches;
     return 0;
   }
@@ -1666,7 +1767,8 @@ struct Engine : EngineBase {
     const int tiles = (npc + kDftTileM - 1) / kDftTileM;
     for (int t0 = 0; t0 < tiles; t0 += 65535) {
       const dim3 grd((nf + kDftTileF - 1) / kDftTileF, std::min(65535, tiles - t0));
-      k_dft_mma<<<grd, 128, 0, s>>>(d_stage, npc, nf, nrows, (int)(r0 % kTB), kTB, d_tw, d_re, d_im, t0 * kDftTileM);
+      k_dft_mma<<<grd, 128, 0, s>>>(d_stage, npc, nf, nrows, (int)(r0 % kStageRows), kStageRows, d_tw, d_re, d_im,
+                                    t0 * kDftTileM);
       stats.kernel_launches += 1;
     }
     stats.kernel_launches += 1;
@@ -1690,6 +1792,13 @@ struct Engine : EngineBase {
     // they are overwritten.
     if (p.num_bin > 0)
       if (int rc = bin_deliver(q)) return rc;
+    // With merged observer sampling each step samples the next one; the
+    // first step of a problem, and a step whose fields were overwritten
+    // after its samples were taken, are sampled here.
+    if (merge_obs && need_sample) {
+      if (int rc = launch_part(P_OBSERVE, 0, &stats.kernel_launches)) return rc;
+      need_sample = false;
+    }
     if (int rc = launch_graphs(m)) return rc;
     step += m;
     // Output rows produced in this block.
@@ -1829,6 +1938,7 @@ struct Engine : EngineBase {
   int write_field(int c, const double *in) override
   {
     CK(cudaStreamSynchronize(s));
+    need_sample = true;
     if (int rc = upload_volume(g.F[c], in)) return rc;
     CK(cudaStreamSynchronize(ss));
     return 0;
@@ -1874,15 +1984,19 @@ struct Engine : EngineBase {
     if (kernel >= 0 && kernel <= 3) return launch_one(kernel);
     if (kernel == VGPU_K_DFT_BLOCK) {
       const uint64_t st = stats.kernel_launches;
-      const int rc = dft_rows(0, kTB);
+      const int rc = dft_rows(0, kTwRows);
       stats.kernel_launches = st;
       return rc;
     }
-    return launch_part(part_of(kernel), 0, nullptr);
+    return launch_step_part(part_of(kernel), 0, nullptr);
   }
 
   int time_kernel(int kernel, int warmup, int iters, double *ms, uint64_t *points) override
   {
+    // Timed launches act at the current step (the counter does not move);
+    // step-indexed tables (source values, the auxiliary grid's drive) have
+    // rows for the problem's steps only.
+    if (step >= p.num_steps) return set_err(VGPU_EINVAL, "kernel timing needs a step inside the problem");
     uint64_t pts = 0;
     if (kernel >= 0 && kernel <= 3) {
       uint64_t bulk_pts = 0, pml_pts = 0;
@@ -1896,7 +2010,7 @@ struct Engine : EngineBase {
     } else {
       const int part = part_of(kernel);
       if (part < 0) return set_err(VGPU_EINVAL, "kernel %d is not a step kernel", kernel);
-      if (!part_present(part)) return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
+      if (!step_part_present(part)) return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
     }
     for (int q = 0; q < warmup; q++)
       if (int rc = launch_timed(kernel)) return rc;

@@ -161,7 +161,7 @@ __global__ void k_mur_h(Grid<T> g, MurView mv, int64_t total)
 }
 
 // ---------------------------------------------------------------------------
-// Debye blocks (src/debye.c:243-307): one thread per (block, component, cell).
+// Debye blocks (src/debye.c:243-307).
 // ---------------------------------------------------------------------------
 
 struct DebyeItem {
@@ -173,20 +173,29 @@ struct DebyeItem {
   int coef_ofs;      // offset of dalpha/dbeta (complex, np each) in coefs
 };
 
+// One (item, cell) of the Debye update, thread index t over all items.  The
+// independent loads (the field, its last value, the update coefficient, the
+// currents) are issued before any arithmetic; the expressions are the
+// reference's: E = E - beta * sum((1 + dalpha) J) rounded once to T, then
+// J = dalpha J + dbeta (E - lastE).
 template <typename T>
-__global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t total, double2 *J, T *lastE,
-                        const double2 *coefs)
+__device__ __forceinline__ void debye_point(const Grid<T> &g, const DebyeItem *__restrict__ items, int nitems,
+                                            int64_t t, double2 *__restrict__ J, T *__restrict__ lastE,
+                                            const double2 *__restrict__ coefs)
 {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
   int q = 0;
   while (q + 1 < nitems && t >= items[q + 1].first) q++;
   const DebyeItem m = items[q];
-  int64_t cell = t - m.first;
-  int64_t nj = m.b.nj(), nk = m.b.nk();
-  int i = m.b.i0 + (int)(cell / (nj * nk)), j = m.b.j0 + (int)((cell / nk) % nj), k = m.b.k0 + (int)(cell % nk);
+  const int64_t cell = t - m.first;
+  const int64_t nj = m.b.nj(), nk = m.b.nk();
+  const int i = m.b.i0 + (int)(cell / (nj * nk)), j = m.b.j0 + (int)((cell / nk) % nj),
+            k = m.b.k0 + (int)(cell % nk);
   const int64_t x = g.at(i, j, k);
   T *E = g.F[m.c];
+  const int64_t le = m.eofs + cell;
+  const T e_old = E[x];
+  const T last = lastE[le];
+  const T beta = g.coef(3 + m.c, x);
   const double2 *da = coefs + m.coef_ofs, *db = da + m.np;
   double2 *Jc = J + m.jofs + cell * m.np;
   // Jsum = sum (1 + dalpha) * J, complex arithmetic as C99 (no contraction).
@@ -197,15 +206,25 @@ __global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t t
     sr = sr + (ar * v.x - ai * v.y);
     si = si + (ar * v.y + ai * v.x);
   }
-  E[x] = E[x] - g.coef(3 + m.c, x) * sr;
-  T diff = E[x] - lastE[m.eofs + cell];
+  const T e_new = e_old - beta * sr;
+  E[x] = e_new;
+  const T diff = e_new - last;
   for (int p = 0; p < m.np; p++) {
     double2 v = Jc[p];
     double nr = (da[p].x * v.x - da[p].y * v.y) + db[p].x * (double)diff;
     double ni = (da[p].x * v.y + da[p].y * v.x) + db[p].y * (double)diff;
     Jc[p] = make_double2(nr, ni);
   }
-  lastE[m.eofs + cell] = E[x];
+  lastE[le] = e_new;
+}
+
+// Debye blocks (src/debye.c:243-307): one thread per (block, component, cell).
+template <typename T>
+__global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t total, double2 *J, T *lastE,
+                        const double2 *coefs)
+{
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < total) debye_point(g, items, nitems, t, J, lastE, coefs);
 }
 
 // ---------------------------------------------------------------------------
@@ -336,13 +355,14 @@ __global__ void k_bin_observe(Grid<T> g, const int *__restrict__ pts, int64_t np
   ring[row * npts * 6 + t] = (float)g.F[c][x];
 }
 
+// Samples of step n at thread t: TD points' six components into the TD
+// buffer (row n - out_start), then FD points' into staging row
+// (n - out_start) % tblock.
 template <typename T>
-__global__ void k_observe(Grid<T> g, const int *td_pts, int num_td, const int *fd_pts, int num_fd, T *td_buf,
-                          double *fd_stage, const uint64_t *step_base, int step_rel, uint64_t out_start,
-                          uint64_t out_stop, int tblock)
+__device__ __forceinline__ void observe_point(const Grid<T> &g, const int *td_pts, int num_td, const int *fd_pts,
+                                              int num_fd, T *td_buf, double *fd_stage, uint64_t n,
+                                              uint64_t out_start, uint64_t out_stop, int tblock, int t)
 {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  uint64_t n = *step_base + step_rel;
   if (n < out_start || n > out_stop) return;
   uint64_t row = n - out_start;
   if (t < num_td * 6) {
@@ -357,6 +377,15 @@ __global__ void k_observe(Grid<T> g, const int *td_pts, int num_td, const int *f
     const int *pt = fd_pts + 3 * p;
     fd_stage[(row % tblock) * (int64_t)num_fd * 6 + t] = (double)g.F[c][g.at(pt[0], pt[1], pt[2])];
   }
+}
+
+template <typename T>
+__global__ void k_observe(Grid<T> g, const int *td_pts, int num_td, const int *fd_pts, int num_fd, T *td_buf,
+                          double *fd_stage, const uint64_t *step_base, int step_rel, uint64_t out_start,
+                          uint64_t out_stop, int tblock)
+{
+  observe_point(g, td_pts, num_td, fd_pts, num_fd, td_buf, fd_stage, *step_base + step_rel, out_start, out_stop,
+                tblock, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // Twiddles cos/sin(omega_f * t_n) for the rows of one DFT block.
@@ -720,13 +749,11 @@ __device__ __forceinline__ T tfsf_apply(const PwView<T> &pw, const TfsfView &tv,
 constexpr int kTfsfPerThread = 2;
 
 template <typename T>
-__global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl, double dt,
-                            const uint64_t *step_base, int step_rel, int efield)
+__device__ __forceinline__ void tfsf_point(const Grid<T> &g, const PwView<T> &pw, const TfsfView &tv,
+                                           const TfsfList<T> &tl, double dt, uint64_t n, int efield, int t)
 {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int ns4 = (tl.nsingle + kTfsfPerThread - 1) / kTfsfPerThread;
   if (t >= ns4 + tl.nmulti) return;
-  const uint64_t n = *step_base + step_rel;
   const double time = efield ? n * dt : (n + 0.5) * dt;
   if (t < ns4) {
     TfsfEntry<T> en[kTfsfPerThread];
@@ -749,6 +776,62 @@ __global__ void k_tfsf_list(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T> tl
   T v = F[first.x];
   for (int e = e0; e < e1; e++) v = tfsf_apply(pw, tv, tl.ent[e], v, time, efield);
   F[first.x] = v;
+}
+
+template <typename T>
+__global__ void k_tfsf_list(Grid<T> g, const __grid_constant__ PwView<T> pw, const __grid_constant__ TfsfView tv,
+                            const __grid_constant__ TfsfList<T> tl, double dt, const uint64_t *step_base,
+                            int step_rel, int efield)
+{
+  tfsf_point(g, pw, tv, tl, dt, *step_base + step_rel, efield, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+}
+
+// Parts of a step that touch disjoint points, run as one launch so their
+// latency-bound chains overlap (the engine checks disjointness at set-up):
+// blocks [0, nb_debye) take the Debye cells, the next nb_tfsf blocks one
+// plane wave's corrections of the step, and the last nb_obs blocks the
+// observer samples of the step after it.  Each job does exactly what its own
+// kernel does (k_debye, k_tfsf_list, k_observe).
+template <typename T>
+struct SideLaunch {
+  int nb_debye, nb_tfsf, nb_obs;
+  const DebyeItem *debye;
+  int n_debye;
+  int64_t debye_total;
+  double2 *J;
+  T *lastE;
+  const double2 *dcoef;
+  PwView<T> pw;
+  TfsfView tv;
+  TfsfList<T> tl;
+  double dt;
+  int efield;
+  const int *td_pts, *fd_pts;
+  int num_td, num_fd;
+  T *td_buf;
+  double *fd_stage;
+  uint64_t out_start, out_stop;
+  int tblock;
+};
+
+template <typename T>
+__global__ void k_side(Grid<T> g, const __grid_constant__ SideLaunch<T> L, const uint64_t *step_base, int step_rel)
+{
+  int b = blockIdx.x;
+  const uint64_t n = *step_base + step_rel;
+  if (b < L.nb_debye) {
+    const int64_t t = (int64_t)b * blockDim.x + threadIdx.x;
+    if (t < L.debye_total) debye_point(g, L.debye, L.n_debye, t, L.J, L.lastE, L.dcoef);
+    return;
+  }
+  b -= L.nb_debye;
+  if (b < L.nb_tfsf) {
+    tfsf_point(g, L.pw, L.tv, L.tl, L.dt, n, L.efield, (int)(b * blockDim.x + threadIdx.x));
+    return;
+  }
+  b -= L.nb_tfsf;
+  observe_point(g, L.td_pts, L.num_td, L.fd_pts, L.num_fd, L.td_buf, L.fd_stage, n + 1, L.out_start, L.out_stop,
+                L.tblock, (int)(b * blockDim.x + threadIdx.x));
 }
 
 // ---------------------------------------------------------------------------
