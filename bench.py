@@ -281,7 +281,7 @@ def error_report(td, re, im, td64, re64, im64, steps, fd_names=None):
                 if r is None:
                     continue
                 for c in range(6):
-                    if not np.isnan(dbm[q, c]) and r[c] == r[c]:
+                    if not np.isnan(dbm[q, c]) and r[c] is not None:
                         mine.append(dbm[q, c])
                         theirs.append(r[c])
             mine, theirs = np.array(mine), np.array(theirs)

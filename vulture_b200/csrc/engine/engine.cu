@@ -255,6 +255,34 @@ static RegionSet regions_of(const vgpu_problem &p)
   return rs;
 }
 
+// The normal H of a Mur face (src/mur.c:401-555) takes the bulk H update
+// (src/grid.c:800-888): the same expression, reading only E, at points the
+// bulk limits leave out.  Where a face's box and its component's bulk box
+// are disjoint and their union is itself a box (the face box extends the
+// bulk box by a plane, as on every outer Mur face), the bulk box grows by
+// it and the face needs no update of its own.  The reference updates Mur H
+// before the bulk H; both read E only and write disjoint points, so the
+// order does not matter.  Returns the bits of the faces absorbed.
+static unsigned fold_mur_h(const vgpu_problem &p, Box bh[3])
+{
+  unsigned folded = 0;
+  for (int pass = 0; pass < 2; pass++)   // a face may extend a box another face already grew
+    for (int f = 0; f < 6; f++) {
+      if (!p.mur_present[f] || (folded >> f & 1u)) continue;
+      const int c = f / 2;                      // the face's normal H component
+      const Box m = box_from(p.mur_flim[f][HX + c]);
+      if (m.empty()) { folded |= 1u << f; continue; }
+      Box &b = bh[c];
+      if (b.empty() || boxes_meet(b, m)) continue;
+      const Box u{ std::min(b.i0, m.i0), std::max(b.i1, m.i1), std::min(b.j0, m.j0), std::max(b.j1, m.j1),
+                   std::min(b.k0, m.k0), std::max(b.k1, m.k1) };
+      if (u.count() != b.count() + m.count()) continue;
+      b = u;
+      folded |= 1u << f;
+    }
+  return folded;
+}
+
 // The tiles of one half step (host only).  Columns of 32 x 8 points, cut
 // into runs of i planes sized so a launch has several tiles per resident
 // block (the pipeline runs across tile boundaries).  Bulk-footprint tiles
@@ -359,7 +387,9 @@ struct Engine : EngineBase {
   PmlView<T> pv{};
   // Mur
   MurView mve{}, mvh{};
+  unsigned mur_h_folded = 0;   // Mur faces whose normal H the H sweep updates (fold_mur_h)
   int64_t mur_total_e = 0, mur_total_h = 0;
+  int64_t mur_max_e = 0, mur_max_h = 0;   // points of the largest item (launch grid x)
   // Debye
   DebyeItem *d_debye = nullptr;
   int n_debye = 0;
@@ -378,7 +408,7 @@ struct Engine : EngineBase {
   int64_t sibc_faces = 0;
   int64_t *d_tgt_index = nullptr, *d_tgt_start = nullptr;
   int *d_tgt_comp = nullptr;
-  SibcOp *d_ops = nullptr;
+  SibcOp<T> *d_ops = nullptr;
   int64_t ntgt = 0;
   // sources and plane waves
   std::vector<SrcLaunch> srcs;
@@ -586,6 +616,8 @@ struct Engine : EngineBase {
     ubh = unite(bh);
 
     if (int rc = setup_pml()) return rc;
+    mur_h_folded = fold_mur_h(p, bh);
+    ubh = unite(bh);
     setup_mur();
     if (int rc = setup_debye()) return rc;
     if (int rc = setup_sibc()) return rc;
@@ -652,12 +684,14 @@ struct Engine : EngineBase {
         MurItem &m = mve.it[mve.nitems++];
         m.b = b; m.c = comps[cc]; m.axis = a; m.dir = dir; m.face = f; m.first = mur_total_e;
         mur_total_e += b.count();
+        mur_max_e = std::max(mur_max_e, b.count());
       }
       Box b = box_from(p.mur_flim[f][HX + a]);
-      if (!b.empty()) {
+      if (!b.empty() && !(mur_h_folded >> f & 1u)) {
         MurItem &m = mvh.it[mvh.nitems++];
         m.b = b; m.c = HX + a; m.axis = a; m.dir = 0; m.face = f; m.first = mur_total_h;
         mur_total_h += b.count();
+        mur_max_h = std::max(mur_max_h, b.count());
       }
     }
   }
@@ -752,10 +786,11 @@ struct Engine : EngineBase {
     CK(cudaMemsetAsync(d_zeta, 0, sizeof(double2) * (z ? z : 1), ss));
     CK(cudaMemsetAsync(d_old, 0, sizeof(double) * (faces ? faces * 16 : 1), ss));
     CK(cudaMemsetAsync(d_etan, 0, sizeof(T) * (faces ? faces * 4 : 1), ss));
+    if (faces * 4 > INT32_MAX) return set_err(VGPU_EINVAL, "%lld SIBC faces exceed the engine's limit", (long long)faces);
     // Magnetic correction targets (ops arrive sorted by target).
     std::vector<int64_t> tidx, tstart;
     std::vector<int> tcomp;
-    std::vector<SibcOp> ops((size_t)p.num_sibc_hops + 1);
+    std::vector<SibcOp<T>> ops((size_t)p.num_sibc_hops + 1);
     for (int64_t h = 0; h < p.num_sibc_hops; h++) {
       const vgpu_sibc_hop &o = p.sibc_hops[h];
       int i = (int)(o.index / ((int64_t)p.n[1] * p.n[2]));
@@ -767,11 +802,11 @@ struct Engine : EngineBase {
         tcomp.push_back(o.comp);
         tstart.push_back(h);
       }
-      SibcOp &d = ops[h];
+      SibcOp<T> &d = ops[h];
       d.kind = o.kind;
-      d.c = o.c; d.d1 = o.d1; d.d2 = o.d2; d.n1 = o.n1; d.n2 = o.n2;
-      d.e1 = 4 * (base[o.s1] + o.f1) + o.slot1;
-      d.e2 = 4 * (base[o.s2] + o.f2) + o.slot2;
+      d.c = (T)o.c; d.d1 = (T)o.d1; d.d2 = (T)o.d2; d.n1 = (T)o.n1; d.n2 = (T)o.n2;
+      d.e1 = (int32_t)(4 * (base[o.s1] + o.f1) + o.slot1);
+      d.e2 = (int32_t)(4 * (base[o.s2] + o.f2) + o.slot2);
     }
     tstart.push_back(p.num_sibc_hops);
     ntgt = (int64_t)tidx.size();
@@ -1529,7 +1564,10 @@ struct Engine : EngineBase {
       // Mur reads the neighbours' pre-update E, so it precedes the sweeps;
       // the PML and bulk sweeps touch disjoint E points.
       case P_MUR_E:
-        if (mve.nitems) { k_mur_e<T><<<blocks_for(mur_total_e, 128), 128, 0, s>>>(g, mve, mur_total_e); launches++; }
+        if (mve.nitems) {
+          k_mur_e<T><<<dim3(blocks_for(mur_max_e, 128), mve.nitems), 128, 0, s>>>(g, mve);
+          launches++;
+        }
         break;
       case P_SWEEP_E:
         if (int rc = launch_sweep_pair(true, &launches)) return rc;
@@ -1575,7 +1613,10 @@ struct Engine : EngineBase {
         }
         break;
       case P_MUR_H:
-        if (mvh.nitems) { k_mur_h<T><<<blocks_for(mur_total_h, 128), 128, 0, s>>>(g, mvh, mur_total_h); launches++; }
+        if (mvh.nitems) {
+          k_mur_h<T><<<dim3(blocks_for(mur_max_h, 128), mvh.nitems), 128, 0, s>>>(g, mvh);
+          launches++;
+        }
         break;
       case P_SWEEP_H:
         if (int rc = launch_sweep_pair(false, &launches)) return rc;
@@ -2155,6 +2196,7 @@ extern "C" int vgpu_check_sweep_plan(const vgpu_problem *p, int32_t precision, i
   for (int es = 0; es < 2; es++) {
     Box bb[3];
     for (int c = 0; c < 3; c++) bb[c] = box_from(p->gfilim[(es ? 0 : 3) + c]);
+    if (!es) fold_mur_h(*p, bb);
     const SweepPlan pl = plan_sweep(unite(bb), rs, es != 0, halo, 148);
     std::vector<SweepTile> all(pl.bulk);
     all.insert(all.end(), pl.pml.begin(), pl.pml.end());

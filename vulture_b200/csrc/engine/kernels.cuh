@@ -122,34 +122,31 @@ __device__ __forceinline__ void item_coords(const MurItem &m, int64_t t, int &i,
   k = m.b.k0 + (int)(t % nk);
 }
 
+// One launch covers every item: blockIdx.y is the item, threads walk its
+// face box (k fastest), so no thread searches the item list.
 template <typename T>
-__global__ void k_mur_e(Grid<T> g, MurView mv, int64_t total)
+__global__ void k_mur_e(Grid<T> g, const __grid_constant__ MurView mv)
 {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  int q = 0;
-  while (q + 1 < mv.nitems && t >= mv.it[q + 1].first) q++;
-  const MurItem &m = mv.it[q];
+  const MurItem &m = mv.it[blockIdx.y];
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.b.count()) return;
   int i, j, k;
-  item_coords<T>(m, t - m.first, i, j, k);
-  int n[3] = { i, j, k };
-  n[m.axis] += m.dir;
-  T tmp = bulk_e_value(g, m.c, n[0], n[1], n[2]);
-  int64_t x = g.at(i, j, k), xn = g.at(n[0], n[1], n[2]);
+  item_coords<T>(m, t, i, j, k);
+  const int ni = i + (m.axis == 0 ? m.dir : 0), nj = j + (m.axis == 1 ? m.dir : 0), nk = k + (m.axis == 2 ? m.dir : 0);
+  T tmp = bulk_e_value(g, m.c, ni, nj, nk);
+  const int64_t x = g.at(i, j, k), xn = g.at(ni, nj, nk);
   T *F = g.F[m.c];
   F[x] = F[xn] + (T)mv.zeta[m.face] * (tmp - F[x]);
 }
 
 template <typename T>
-__global__ void k_mur_h(Grid<T> g, MurView mv, int64_t total)
+__global__ void k_mur_h(Grid<T> g, const __grid_constant__ MurView mv)
 {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  int q = 0;
-  while (q + 1 < mv.nitems && t >= mv.it[q + 1].first) q++;
-  const MurItem &m = mv.it[q];
+  const MurItem &m = mv.it[blockIdx.y];
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.b.count()) return;
   int i, j, k;
-  item_coords<T>(m, t - m.first, i, j, k);
+  item_coords<T>(m, t, i, j, k);
   const int64_t x = g.at(i, j, k);
   const T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
   if (m.c == HX)
@@ -905,6 +902,13 @@ __global__ void k_sibc_e(Grid<T> g, const SibcSurf *surfs, int nsurf, const Sibc
       double y = m.asymp[a][b] * xin;
       int off = m.off[a][b];
       double2 *zz = z + (off - m.off[0][0]);
+      // A filter entry without poles is its constant term alone: its input
+      // history feeds only the pole recursion, so it is neither read nor
+      // kept (nothing else reads it).
+      if (m.np[a][b] == 0) {
+        Eout[a] = Eout[a] + y;
+        continue;
+      }
       double po = o[4 * a + b];
       for (int r = 0; r < m.np[a][b]; r++) {
         double2 a0 = q0[off + r], a1 = q1[off + r], a2 = q2[off + r], zv = zz[r];
@@ -927,16 +931,21 @@ __global__ void k_sibc_e(Grid<T> g, const SibcSurf *surfs, int nsurf, const Sibc
   }
 }
 
-// One thread per corrected H value: apply its operations in order.
+// One thread per corrected H value: apply its operations in order.  The
+// operation's coefficients are stored in T, the type the correction
+// computes in (the values are rounded to T once, at set-up, where the
+// update rounded them at each use), and its tangential-E indices in 32 bits.
+template <typename T>
 struct SibcOp {
-  int64_t e1, e2;     // indices into etan
-  double c, d1, d2, n1, n2;
-  int kind, pad;
+  int32_t e1, e2;     // indices into etan
+  int32_t kind, pad;
+  T c, d1, d2, n1, n2;
 };
 
 template <typename T>
-__global__ void k_sibc_h(Grid<T> g, const int64_t *tgt_index, const int *tgt_comp, const int64_t *tgt_start,
-                         int64_t ntgt, const SibcOp *ops, const T *etan)
+__global__ void k_sibc_h(Grid<T> g, const int64_t *__restrict__ tgt_index, const int *__restrict__ tgt_comp,
+                         const int64_t *__restrict__ tgt_start, int64_t ntgt, const SibcOp<T> *__restrict__ ops,
+                         const T *__restrict__ etan)
 {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntgt) return;
@@ -944,15 +953,14 @@ __global__ void k_sibc_h(Grid<T> g, const int64_t *tgt_index, const int *tgt_com
   const int64_t x = tgt_index[t];
   T h = F[x];
   for (int64_t q = tgt_start[t]; q < tgt_start[t + 1]; q++) {
-    const SibcOp o = ops[q];
+    const SibcOp<T> o = ops[q];
     if (o.kind == 0) { h = 0.0; continue; }
-    T c = (T)o.c, d1 = (T)o.d1;
-    T e1 = etan[o.e1];
+    const T e1 = etan[o.e1];
     if (o.kind == 1) {
-      h = h + c * (d1 * e1);
+      h = h + o.c * (o.d1 * e1);
     } else {
-      T e2 = etan[o.e2], d2 = (T)o.d2, n1 = (T)o.n1, n2 = (T)o.n2;
-      h = h + c * (n1 * (d1 * e1) + n2 * (d2 * e2));
+      const T e2 = etan[o.e2];
+      h = h + o.c * (o.n1 * (o.d1 * e1) + o.n2 * (o.d2 * e2));
     }
   }
   F[x] = h;
