@@ -361,7 +361,11 @@ enum { VGPU_K_BULK_E = 0, VGPU_K_BULK_H = 1, VGPU_K_PML_E = 2, VGPU_K_PML_H = 3 
 enum {
   VGPU_K_OBSERVE = 4, VGPU_K_BIN_OBSERVE = 5, VGPU_K_MUR_E = 6, VGPU_K_DEBYE = 7, VGPU_K_SIBC_E = 8,
   VGPU_K_SOURCES_E = 9, VGPU_K_TFSF_E = 10, VGPU_K_GHOST_E = 11, VGPU_K_MUR_H = 12, VGPU_K_SIBC_H = 13,
-  VGPU_K_SOURCES_H = 14, VGPU_K_TFSF_H = 15, VGPU_K_GHOST_H = 16, VGPU_K_DFT_BLOCK = 17
+  VGPU_K_SOURCES_H = 14, VGPU_K_TFSF_H = 15, VGPU_K_GHOST_H = 16, VGPU_K_DFT_BLOCK = 17,
+  /* Timing only, never part of a step: the same 64-row DFT fold by the
+   * scalar kernel (one thread per point-component and frequency) that the
+   * engine's tensor-core fold replaced, for comparison. */
+  VGPU_K_DFT_BLOCK_SCALAR = 18
 };
 
 /* Field points one sweep kernel updates per launch with the bulk formula

@@ -132,3 +132,5 @@ STEP_KERNELS = {
     "k_tfsf(E)": 10, "k_ghost(E)": 11, "k_mur_h": 12, "k_sibc_h": 13, "k_source(H)": 14, "k_tfsf(H)": 15,
     "k_ghost(H)": 16, "dft_fold_64": 17,
 }
+# Timing only: the scalar DFT fold the tensor-core fold replaced.
+VGPU_K_DFT_BLOCK_SCALAR = 18

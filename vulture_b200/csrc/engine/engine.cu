@@ -423,6 +423,7 @@ struct Engine : EngineBase {
   double *d_stage = nullptr, *d_re = nullptr, *d_im = nullptr, *d_omega = nullptr;
   double2 *d_tw = nullptr;
   uint64_t nout = 0;
+  uint64_t dft_folded = 0;   // output rows already folded into d_re/d_im
   // binary observers: device ring of 2 blocks x kChunk rows, pinned host copy
   int *d_bin_pts = nullptr;
   float *d_bin = nullptr, *h_bin = nullptr;
@@ -1847,12 +1848,30 @@ struct Engine : EngineBase {
     if (p.num_bin > 0 && bin_sink && hi >= lo && lo <= p.out_stop) {
       if (int rc = bin_enqueue(q, lo, hi)) return rc;
     }
-    if (p.num_fd && hi >= lo) {
-      if (int rc = dft_rows(lo - p.out_start, hi - p.out_start + 1)) return rc;
-    }
+    // The staged rows are folded into the running DFT once their 64-step
+    // chunk is complete (or the problem ends); rows of a chunk that a run
+    // leaves unfinished are folded with the rest of the chunk, or when the
+    // DFT is read.  A fold costs about the same for 20 rows as for 64 (it
+    // reads and writes every running sum), so partial chunks are not folded
+    // early.
+    if (p.num_fd && (step % kChunk == 0 || step == p.num_steps))
+      if (int rc = fold_pending()) return rc;
+    (void)hi;
     if (step % kChunk == 0 || step == p.num_steps)
       if (int rc = queue_energy()) return rc;
     *queued = m;
+    return 0;
+  }
+
+  // Fold every staged output row of the steps run so far that is not yet in
+  // the running DFT (at most one chunk: folds happen at every chunk end).
+  int fold_pending()
+  {
+    if (!p.num_fd || step <= p.out_start) return 0;
+    const uint64_t staged = std::min<uint64_t>(step - 1, out_last()) - p.out_start + 1;
+    if (staged <= dft_folded) return 0;
+    if (int rc = dft_rows(dft_folded, staged)) return rc;
+    dft_folded = staged;
     return 0;
   }
 
@@ -1960,6 +1979,8 @@ struct Engine : EngineBase {
   {
     size_t n = (size_t)p.num_fd * 6 * p.num_freq;
     if (!n) return 0;
+    if (int rc = fold_pending()) return rc;
+    CK(cudaStreamSynchronize(s));
     CK(cudaMemcpy(re, d_re, sizeof(double) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(im, d_im, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return 0;
@@ -2029,6 +2050,16 @@ struct Engine : EngineBase {
       stats.kernel_launches = st;
       return rc;
     }
+    if (kernel == VGPU_K_DFT_BLOCK_SCALAR) {
+      const int nf = p.num_freq, npc = p.num_fd * 6;
+      k_twiddle<<<blocks_for((int64_t)kTwRows * nf, 128), 128, 0, s>>>(d_omega, nf, p.dt, p.out_start, 0, kTwRows,
+                                                                       d_tw);
+      const dim3 blk(32, 8), grd((nf + 31) / 32, (npc + 7) / 8);
+      if (grd.y > 65535) return set_err(VGPU_EINVAL, "%d point-components exceed the scalar fold's grid", npc);
+      k_dft_accumulate<<<grd, blk, sizeof(double) * 8 * kTwRows, s>>>(d_stage, npc, nf, kTwRows, 0, kStageRows, d_tw,
+                                                                     d_re, d_im);
+      return 0;
+    }
     return launch_step_part(part_of(kernel), 0, nullptr);
   }
 
@@ -2046,7 +2077,7 @@ struct Engine : EngineBase {
       const bool es = kernel == VGPU_K_BULK_E || kernel == VGPU_K_PML_E;
       if (!(es ? sw_e : sw_h)[(kernel == VGPU_K_BULK_E || kernel == VGPU_K_BULK_H) ? 0 : 1].ntiles)
         return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
-    } else if (kernel == VGPU_K_DFT_BLOCK) {
+    } else if (kernel == VGPU_K_DFT_BLOCK || kernel == VGPU_K_DFT_BLOCK_SCALAR) {
       if (!p.num_fd) return set_err(VGPU_EINVAL, "kernel %d not present in this problem", kernel);
     } else {
       const int part = part_of(kernel);

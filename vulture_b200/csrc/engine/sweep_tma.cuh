@@ -451,7 +451,9 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
           if (sel & 4u) F2[x] = v2 + cf[2] * c2;
         }
       }
-      if (PML) {
+      // Bulk-only tiles (reg[0] < 0, the same for the whole block) skip the
+      // UPML part, profile shuffles included.
+      if (PML && t.reg[0] >= 0) {
         const T xa = __shfl_sync(0xffffffffu, pa_l, p), xb = __shfl_sync(0xffffffffu, pb_l, p);
         const T xc = __shfl_sync(0xffffffffu, pc_l, p), xd = __shfl_sync(0xffffffffu, pd_l, p);
         if (ESWEEP) {
