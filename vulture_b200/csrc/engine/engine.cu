@@ -125,6 +125,94 @@ static BlockCache &block_cache()
   return *c;
 }
 
+// Pinned host staging for large host<->device copies.  Copies from and to
+// pageable memory run at a fraction of the link's speed (the driver stages
+// them itself); here they go through two pinned chunks, the DMA of one
+// overlapping the host copy of the other.  One pair serves the process
+// (portable across devices), under a lock; it is allocated by the first
+// engine that needs it and kept until exit.
+struct PinnedStage {
+  static constexpr size_t kChunkBytes = 8u << 20;
+  std::mutex mu;
+  char *buf = nullptr;
+
+  int ensure()
+  {
+    if (buf) return 0;
+    CK(cudaHostAlloc((void **)&buf, 2 * kChunkBytes, cudaHostAllocPortable));
+    return 0;
+  }
+
+  // Device -> host: chunk q lands in half q % 2; while it is copied out on
+  // the host, chunk q + 1 is in flight.
+  int d2h(void *dst, const void *src, size_t bytes, cudaStream_t st)
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (int rc = ensure()) return rc;
+    cudaEvent_t ev[2];
+    CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    const size_t nchunks = (bytes + kChunkBytes - 1) / kChunkBytes;
+    cudaError_t e = cudaSuccess;
+    auto issue = [&](size_t q) {
+      const size_t off = q * kChunkBytes, n = std::min(kChunkBytes, bytes - off);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf + (q % 2) * kChunkBytes, (const char *)src + off, n, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev[q % 2], st);
+    };
+    if (nchunks) issue(0);
+    for (size_t q = 0; q < nchunks && e == cudaSuccess; q++) {
+      if (q + 1 < nchunks) issue(q + 1);
+      if (e == cudaSuccess) e = cudaEventSynchronize(ev[q % 2]);
+      if (e != cudaSuccess) break;
+      const size_t off = q * kChunkBytes, n = std::min(kChunkBytes, bytes - off);
+      memcpy((char *)dst + off, buf + (q % 2) * kChunkBytes, n);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // nothing of ours left in flight
+    else cudaStreamSynchronize(st);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (e != cudaSuccess) return set_err(VGPU_ECUDA, "staged device-to-host copy: %s", cudaGetErrorString(e));
+    return 0;
+  }
+
+  // Host -> device: the host fills half q % 2 once chunk q - 2's DMA out of
+  // it has finished; returns after the last chunk has landed.
+  int h2d(void *dst, const void *src, size_t bytes, cudaStream_t st)
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (int rc = ensure()) return rc;
+    cudaEvent_t ev[2];
+    CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    const size_t nchunks = (bytes + kChunkBytes - 1) / kChunkBytes;
+    cudaError_t e = cudaSuccess;
+    for (size_t q = 0; q < nchunks && e == cudaSuccess; q++) {
+      if (q >= 2) e = cudaEventSynchronize(ev[q % 2]);
+      if (e != cudaSuccess) break;
+      const size_t off = q * kChunkBytes, n = std::min(kChunkBytes, bytes - off);
+      memcpy(buf + (q % 2) * kChunkBytes, (const char *)src + off, n);
+      e = cudaMemcpyAsync((char *)dst + off, buf + (q % 2) * kChunkBytes, n, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev[q % 2], st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    else cudaStreamSynchronize(st);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (e != cudaSuccess) return set_err(VGPU_ECUDA, "staged host-to-device copy: %s", cudaGetErrorString(e));
+    return 0;
+  }
+};
+
+static PinnedStage &pinned_stage()
+{
+  static PinnedStage *st = new PinnedStage;   // never destroyed: outlives every engine
+  return *st;
+}
+
+// Copies at least this large go through the pinned stage.
+static const size_t kStagedCopyBytes = 1u << 20;
+
 struct DevAlloc {
   struct Block {
     void *p;
@@ -490,7 +578,11 @@ struct Engine : EngineBase {
   int upload(U **d, const U *h, size_t n)
   {
     if (mem.alloc(d, n)) return VGPU_ENOMEM;
-    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
+    if (sizeof(U) * n >= kStagedCopyBytes) {
+      if (int rc = pinned_stage().h2d(*d, h, sizeof(U) * n, ss)) return rc;
+    } else if (n) {
+      CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
+    }
     stats.h2d_bytes += sizeof(U) * n;
     return 0;
   }
@@ -502,7 +594,11 @@ struct Engine : EngineBase {
     std::vector<T> tmp(n + pad ? n + pad : 1, (T)0);
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
     if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
-    if (n + pad) CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
+    if (sizeof(T) * (n + pad) >= kStagedCopyBytes) {
+      if (int rc = pinned_stage().h2d(*d, tmp.data(), sizeof(T) * (n + pad), ss)) return rc;
+    } else if (n + pad) {
+      CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
+    }
     stats.h2d_bytes += sizeof(T) * (n + pad);
     return 0;
   }
@@ -517,7 +613,7 @@ struct Engine : EngineBase {
         T *dst = tmp.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
         for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
       }
-    CK(cudaMemcpyAsync(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice, ss));
+    if (int rc = pinned_stage().h2d(d, tmp.data(), sizeof(T) * vol, ss)) return rc;
     stats.h2d_bytes += sizeof(T) * vol;
     return 0;
   }
@@ -1970,7 +2066,10 @@ struct Engine : EngineBase {
   {
     size_t n = (size_t)std::min<uint64_t>(steps, nout) * p.num_td * 6;
     std::vector<T> tmp(n ? n : 1);
-    if (n) CK(cudaMemcpy(tmp.data(), d_td, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    if (n) {
+      CK(cudaStreamSynchronize(s));
+      if (int rc = pinned_stage().d2h(tmp.data(), d_td, sizeof(T) * n, s)) return rc;
+    }
     for (size_t q = 0; q < n; q++) out[q] = (double)tmp[q];
     return 0;
   }
@@ -1981,15 +2080,16 @@ struct Engine : EngineBase {
     if (!n) return 0;
     if (int rc = fold_pending()) return rc;
     CK(cudaStreamSynchronize(s));
-    CK(cudaMemcpy(re, d_re, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(im, d_im, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (int rc = pinned_stage().d2h(re, d_re, sizeof(double) * n, s)) return rc;
+    if (int rc = pinned_stage().d2h(im, d_im, sizeof(double) * n, s)) return rc;
     return 0;
   }
 
   int read_field(int c, double *out) override
   {
     std::vector<T> tmp((size_t)vol);
-    CK(cudaMemcpy(tmp.data(), g.F[c], sizeof(T) * vol, cudaMemcpyDeviceToHost));
+    CK(cudaStreamSynchronize(s));
+    if (int rc = pinned_stage().d2h(tmp.data(), g.F[c], sizeof(T) * vol, s)) return rc;
     for (int i = 0; i < p.n[0]; i++)
       for (int j = 0; j < p.n[1]; j++)
         for (int k = 0; k < p.n[2]; k++)

@@ -469,21 +469,25 @@ __global__ void __launch_bounds__(128) k_dft_mma(const double *__restrict__ stag
   double acc[8][4];
 #pragma unroll
   for (int ni = 0; ni < 8; ni++) acc[ni][0] = acc[ni][1] = acc[ni][2] = acc[ni][3] = 0.0;
+  // Each thread loads the same tile column c of rows r = tid / 64 + 2q (A)
+  // and tid / 32 + 4q (B): the ring row is found once per row, not per value.
+  const int ca = tid % kDftTileM, cb = tid % kDftTileF;
   for (int r0 = 0; r0 < nrows; r0 += kDftTileK) {
     const int kr = min(kDftTileK, nrows - r0);
-    for (int q = tid; q < kDftTileK * kDftTileM; q += 128) {
-      const int r = q / kDftTileM, c = q % kDftTileM, pc = m0 + c;
-      As[r][c] = (r < kr && pc < npc) ? stage[(int64_t)((row_offset + r0 + r) % tblock) * npc + pc] : 0.0;
+    for (int r = tid / kDftTileM; r < kDftTileK; r += 128 / kDftTileM) {
+      const int pc = m0 + ca;
+      As[r][ca] = (r < kr && pc < npc) ? stage[(int64_t)((row_offset + r0 + r) % tblock) * npc + pc] : 0.0;
     }
-    for (int q = tid; q < kDftTileK * kDftTileF; q += 128) {
-      const int r = q / kDftTileF, c = q % kDftTileF, f = f0 + c;
+    for (int r = tid / kDftTileF; r < kDftTileK; r += 128 / kDftTileF) {
+      const int f = f0 + cb;
       const double2 w = (r < kr && f < nf) ? tw[(int64_t)(r0 + r) * nf + f] : make_double2(0.0, 0.0);
-      Bs[r][2 * c] = w.x;
-      Bs[r][2 * c + 1] = -w.y;
+      Bs[r][2 * cb] = w.x;
+      Bs[r][2 * cb + 1] = -w.y;
     }
     __syncthreads();
-    const int kp = (kr + 3) & ~3;
-    for (int k = 0; k < kp; k += 4) {
+    // A full pass of kDftTileK rows, unrolled; rows past nrows are zeros.
+#pragma unroll
+    for (int k = 0; k < kDftTileK; k += 4) {
       const double a0 = As[k + t][16 * warp + g], a1 = As[k + t][16 * warp + g + 8];
       double b[8];
 #pragma unroll
