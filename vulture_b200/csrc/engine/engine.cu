@@ -119,20 +119,58 @@ static int host_threads()
   return std::max(1, std::min(32, hw / busy));
 }
 
+// Run fn(lo, hi) over [0, n) split into contiguous ranges on up to
+// host_threads() threads (the calling thread takes the first range).
+template <typename F>
+static void parallel_ranges(size_t n, F fn, size_t min_per_thread = 256)
+{
+  const size_t nthr = std::max<size_t>(1, std::min<size_t>((size_t)host_threads(), n / min_per_thread));
+  if (nthr <= 1) {
+    fn((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t w = 1; w < nthr; w++) pool.emplace_back(fn, n * w / nthr, n * (w + 1) / nthr);
+  fn((size_t)0, n / nthr);
+  for (auto &t : pool) t.join();
+}
+
 static BlockCache &block_cache()
 {
   static BlockCache *c = new BlockCache();   // never destroyed: it may outlive the CUDA runtime at exit
   return *c;
 }
 
-// Pinned host staging for large host<->device copies.  Copies from and to
-// pageable memory run at a fraction of the link's speed (the driver stages
-// them itself); here they go through two pinned chunks, the DMA of one
-// overlapping the host copy of the other.  One pair serves the process
+// Pinned host staging for large device-to-host reads.  A read into pageable
+// memory runs at a fraction of the link's speed (the driver stages it
+// itself, one core copying into freshly faulted pages); here it goes
+// through two pinned chunks, the DMA of one overlapping the host copy of the
+// other, which runs on several threads.  (Uploads at creation stay plain
+// asynchronous copies: staging them needs a stream synchronisation per copy,
+// which made creating 256 batch engines 3.4x slower.)  One pair serves the process
 // (portable across devices), under a lock; it is allocated by the first
 // engine that needs it and kept until exit.
+// Host copy of n bytes on up to 8 threads (large copies into fresh pages
+// are bound by page faults and one core's copy rate).
+static void host_copy(void *dst, const void *src, size_t n)
+{
+  const size_t parts = std::min<size_t>(8, std::max<size_t>(1, n >> 21));   // 2 MB or more per thread
+  if (parts <= 1) {
+    memcpy(dst, src, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t w = 1; w < parts; w++)
+    pool.emplace_back([=] {
+      const size_t a = n * w / parts, b = n * (w + 1) / parts;
+      memcpy((char *)dst + a, (const char *)src + a, b - a);
+    });
+  memcpy(dst, src, n / parts);
+  for (auto &t : pool) t.join();
+}
+
 struct PinnedStage {
-  static constexpr size_t kChunkBytes = 8u << 20;
+  static constexpr size_t kChunkBytes = 32u << 20;
   std::mutex mu;
   char *buf = nullptr;
 
@@ -166,7 +204,7 @@ struct PinnedStage {
       if (e == cudaSuccess) e = cudaEventSynchronize(ev[q % 2]);
       if (e != cudaSuccess) break;
       const size_t off = q * kChunkBytes, n = std::min(kChunkBytes, bytes - off);
-      memcpy((char *)dst + off, buf + (q % 2) * kChunkBytes, n);
+      host_copy((char *)dst + off, buf + (q % 2) * kChunkBytes, n);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // nothing of ours left in flight
     else cudaStreamSynchronize(st);
@@ -176,32 +214,6 @@ struct PinnedStage {
     return 0;
   }
 
-  // Host -> device: the host fills half q % 2 once chunk q - 2's DMA out of
-  // it has finished; returns after the last chunk has landed.
-  int h2d(void *dst, const void *src, size_t bytes, cudaStream_t st)
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (int rc = ensure()) return rc;
-    cudaEvent_t ev[2];
-    CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-    const size_t nchunks = (bytes + kChunkBytes - 1) / kChunkBytes;
-    cudaError_t e = cudaSuccess;
-    for (size_t q = 0; q < nchunks && e == cudaSuccess; q++) {
-      if (q >= 2) e = cudaEventSynchronize(ev[q % 2]);
-      if (e != cudaSuccess) break;
-      const size_t off = q * kChunkBytes, n = std::min(kChunkBytes, bytes - off);
-      memcpy(buf + (q % 2) * kChunkBytes, (const char *)src + off, n);
-      e = cudaMemcpyAsync((char *)dst + off, buf + (q % 2) * kChunkBytes, n, cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ev[q % 2], st);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    else cudaStreamSynchronize(st);
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    if (e != cudaSuccess) return set_err(VGPU_ECUDA, "staged host-to-device copy: %s", cudaGetErrorString(e));
-    return 0;
-  }
 };
 
 static PinnedStage &pinned_stage()
@@ -209,9 +221,6 @@ static PinnedStage &pinned_stage()
   static PinnedStage *st = new PinnedStage;   // never destroyed: outlives every engine
   return *st;
 }
-
-// Copies at least this large go through the pinned stage.
-static const size_t kStagedCopyBytes = 1u << 20;
 
 struct DevAlloc {
   struct Block {
@@ -578,11 +587,7 @@ struct Engine : EngineBase {
   int upload(U **d, const U *h, size_t n)
   {
     if (mem.alloc(d, n)) return VGPU_ENOMEM;
-    if (sizeof(U) * n >= kStagedCopyBytes) {
-      if (int rc = pinned_stage().h2d(*d, h, sizeof(U) * n, ss)) return rc;
-    } else if (n) {
-      CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
-    }
+    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
     stats.h2d_bytes += sizeof(U) * n;
     return 0;
   }
@@ -594,11 +599,7 @@ struct Engine : EngineBase {
     std::vector<T> tmp(n + pad ? n + pad : 1, (T)0);
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
     if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
-    if (sizeof(T) * (n + pad) >= kStagedCopyBytes) {
-      if (int rc = pinned_stage().h2d(*d, tmp.data(), sizeof(T) * (n + pad), ss)) return rc;
-    } else if (n + pad) {
-      CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
-    }
+    if (n + pad) CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
     stats.h2d_bytes += sizeof(T) * (n + pad);
     return 0;
   }
@@ -613,7 +614,7 @@ struct Engine : EngineBase {
         T *dst = tmp.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
         for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
       }
-    if (int rc = pinned_stage().h2d(d, tmp.data(), sizeof(T) * vol, ss)) return rc;
+    CK(cudaMemcpyAsync(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice, ss));
     stats.h2d_bytes += sizeof(T) * vol;
     return 0;
   }
@@ -1101,20 +1102,29 @@ struct Engine : EngineBase {
       nm += pt.multi.size();
     }
     const size_t ne = ns + nm;
-    std::vector<TfsfEntry<T>> ent;
-    std::vector<int> pos, mstart;
-    ent.reserve(ne);
-    pos.reserve(3 * ne);
-    for (const Part &pt : parts) {
-      ent.insert(ent.end(), pt.single.begin(), pt.single.end());
-      pos.insert(pos.end(), pt.spos.begin(), pt.spos.end());
+    // Each part's runs go to their final offsets, one host thread per part.
+    std::vector<size_t> soff(tv.n + 1, 0), moff(tv.n + 1, ns);
+    for (int q = 0; q < tv.n; q++) {
+      soff[q + 1] = soff[q] + parts[q].single.size();
+      moff[q + 1] = moff[q] + parts[q].multi.size();
     }
-    for (const Part &pt : parts) {
-      const int base = (int)ent.size();
-      for (int m : pt.mstart) mstart.push_back(base + m);
-      ent.insert(ent.end(), pt.multi.begin(), pt.multi.end());
-      pos.insert(pos.end(), pt.mpos.begin(), pt.mpos.end());
+    std::vector<TfsfEntry<T>> ent(ne);
+    std::vector<int> pos(3 * ne), mstart;
+    {
+      auto place = [&](int q) {
+        const Part &pt = parts[q];
+        std::copy(pt.single.begin(), pt.single.end(), ent.begin() + soff[q]);
+        std::copy(pt.spos.begin(), pt.spos.end(), pos.begin() + 3 * soff[q]);
+        std::copy(pt.multi.begin(), pt.multi.end(), ent.begin() + moff[q]);
+        std::copy(pt.mpos.begin(), pt.mpos.end(), pos.begin() + 3 * moff[q]);
+      };
+      std::vector<std::thread> pool;
+      for (int q = 1; q < tv.n; q++) pool.emplace_back(place, q);
+      if (tv.n > 0) place(0);
+      for (auto &t : pool) t.join();
     }
+    for (int q = 0; q < tv.n; q++)
+      for (int m : parts[q].mstart) mstart.push_back((int)moff[q] + m);
     mstart.push_back((int)ne);
     mark("merge");
     tl.nentries = (int64_t)ne;
@@ -1328,7 +1338,9 @@ struct Engine : EngineBase {
       return m;
     };
     auto at = [&](const double *a, int axis, int v) { return (a && v >= 0 && v < p.n[axis]) ? (T)a[v] : (T)0; };
-    for (size_t q = 0; q < tiles.size(); q++) {
+    // Tiles are independent: host threads take contiguous ranges.
+    parallel_ranges(tiles.size(), [&](size_t q0, size_t q1) {
+    for (size_t q = q0; q < q1; q++) {
       const SweepTile &t = tiles[q];
       Hdr &h = hv[q];
       memset(&h, 0, sizeof h);
@@ -1356,6 +1368,7 @@ struct Engine : EngineBase {
           for (int a = 0; a < 4; a++) h.pz[a][c] = at(prof[a][2], 2, k);
       }
     }
+    });
     Hdr *d = nullptr;
     if (upload(&d, hv.data(), hv.size())) return VGPU_ENOMEM;
     L.headers = d;

@@ -215,14 +215,17 @@ class GpuRun:
 
     def dft(self):
         m = self.mesh
-        re = np.zeros((max(m.num_fd, 1), 6, max(m.num_freq, 1)))
-        im = np.zeros_like(re)
-        if m.num_fd:
-            N.check_gpu(N.lib().vgpu_read_dft(self._e, re.ctypes.data, im.ctypes.data))
+        if not m.num_fd or not m.num_freq:
+            z = np.zeros((max(m.num_fd, 1), 6, max(m.num_freq, 1)))
+            return z, z.copy()
+        # Filled entirely by the read: no zero-fill of a buffer about to be overwritten.
+        re = np.empty((m.num_fd, 6, max(m.num_freq, 1)))
+        im = np.empty_like(re)
+        N.check_gpu(N.lib().vgpu_read_dft(self._e, re.ctypes.data, im.ctypes.data))
         return re, im
 
     def field(self, comp: int, shape):
-        out = np.zeros(shape)
+        out = np.empty(shape)
         N.check_gpu(N.lib().vgpu_read_field(self._e, comp, out.ctypes.data))
         return out
 
