@@ -145,7 +145,8 @@ static BlockCache &block_cache()
 // memory runs at a fraction of the link's speed (the driver stages it
 // itself, one core copying into freshly faulted pages); here it goes
 // through two pinned chunks, the DMA of one overlapping the host copy of the
-// other, which runs on several threads.  (Uploads at creation stay plain
+// other, which runs on several threads.  The first engine created pins the
+// chunks, once per process.  (Uploads at creation stay plain
 // asynchronous copies: staging them needs a stream synchronisation per copy,
 // which made creating 256 batch engines 3.4x slower.)  One pair serves the process
 // (portable across devices), under a lock; it is allocated by the first
@@ -170,9 +171,15 @@ static void host_copy(void *dst, const void *src, size_t n)
 }
 
 struct PinnedStage {
-  static constexpr size_t kChunkBytes = 32u << 20;
+  static constexpr size_t kChunkBytes = 16u << 20;
   std::mutex mu;
   char *buf = nullptr;
+
+  int ensure_locked()
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    return ensure();
+  }
 
   int ensure()
   {
@@ -716,7 +723,7 @@ struct Engine : EngineBase {
     if (int rc = setup_pml()) return rc;
     mur_h_folded = fold_mur_h(p, bh);
     ubh = unite(bh);
-    setup_mur();
+    if (int rc = setup_mur()) return rc;
     if (int rc = setup_debye()) return rc;
     if (int rc = setup_sibc()) return rc;
     if (int rc = setup_sources()) return rc;
@@ -728,6 +735,9 @@ struct Engine : EngineBase {
     pc.mark("observers");
     if (int rc = setup_sweeps()) return rc;
     plan_side_merges();
+    // The read-back stage is pinned once per process, by the first engine
+    // created, so no read pays for it.
+    if (int rc = pinned_stage().ensure_locked()) return rc;
     CK(cudaStreamSynchronize(ss));
     CK(cudaGetLastError());
     pc.mark("sweeps");
@@ -763,7 +773,7 @@ struct Engine : EngineBase {
     return 0;
   }
 
-  void setup_mur()
+  int setup_mur()
   {
     mve.nitems = mvh.nitems = 0;
     mur_total_e = mur_total_h = 0;
@@ -792,6 +802,10 @@ struct Engine : EngineBase {
         mur_max_h = std::max(mur_max_h, b.count());
       }
     }
+    if (std::max(mur_max_e, mur_max_h) >= ((int64_t)1 << 31))
+      return set_err(VGPU_EINVAL, "a Mur face of %lld points exceeds the engine's limit",
+                     (long long)std::max(mur_max_e, mur_max_h));
+    return 0;
   }
 
   int setup_debye()
@@ -809,6 +823,8 @@ struct Engine : EngineBase {
         if (bx.empty()) continue;
         DebyeItem it{};
         it.b = bx; it.c = c; it.np = d.num_poles; it.first = total; it.jofs = jtot; it.eofs = etot; it.coef_ofs = ofs;
+        if (bx.count() >= ((int64_t)1 << 31))
+          return set_err(VGPU_EINVAL, "a Debye block of %lld cells exceeds the engine's limit", (long long)bx.count());
         items.push_back(it);
         total += bx.count();
         jtot += bx.count() * d.num_poles;
@@ -867,6 +883,8 @@ struct Engine : EngineBase {
       memcpy(o.A, sf.A, sizeof o.A);
       memcpy(o.B, sf.B, sizeof o.B);
       int64_t nf = o.g.count();
+      if (nf >= ((int64_t)1 << 31))
+        return set_err(VGPU_EINVAL, "an SIBC surface of %lld faces exceeds the engine's limit", (long long)nf);
       base[q] = faces;
       zofs[q] = z;
       adjA.insert(adjA.end(), sf.adjA, sf.adjA + 4 * nf);

@@ -113,13 +113,16 @@ __device__ __forceinline__ T bulk_e_value(const Grid<T> &g, int c, int i, int j,
   return g.coef(2, x) * g.F[EZ][x] + g.coef(5, x) * (g.idh[0][i] * (Hy[x] - Hy[x - g.s0]) + g.idh[1][j] * (Hx[x - g.s1] - Hx[x]));
 }
 
+// A Mur item is one face plane (fewer than 2^31 points, checked at set-up):
+// its coordinates decode in 32-bit arithmetic.
 template <typename T>
 __device__ __forceinline__ void item_coords(const MurItem &m, int64_t t, int &i, int &j, int &k)
 {
-  int64_t nj = m.b.nj(), nk = m.b.nk();
-  i = m.b.i0 + (int)(t / (nj * nk));
-  j = m.b.j0 + (int)((t / nk) % nj);
-  k = m.b.k0 + (int)(t % nk);
+  const unsigned nj = (unsigned)m.b.nj(), nk = (unsigned)m.b.nk(), u = (unsigned)t;
+  const unsigned q = u / nk, r = q / nj;
+  k = m.b.k0 + (int)(u - q * nk);
+  j = m.b.j0 + (int)(q - r * nj);
+  i = m.b.i0 + (int)r;
 }
 
 // One launch covers every item: blockIdx.y is the item, threads walk its
@@ -184,9 +187,10 @@ __device__ __forceinline__ void debye_point(const Grid<T> &g, const DebyeItem *_
   while (q + 1 < nitems && t >= items[q + 1].first) q++;
   const DebyeItem m = items[q];
   const int64_t cell = t - m.first;
-  const int64_t nj = m.b.nj(), nk = m.b.nk();
-  const int i = m.b.i0 + (int)(cell / (nj * nk)), j = m.b.j0 + (int)((cell / nk) % nj),
-            k = m.b.k0 + (int)(cell % nk);
+  // A block holds fewer than 2^31 cells (checked at set-up): 32-bit decode.
+  const unsigned nj = (unsigned)m.b.nj(), nk = (unsigned)m.b.nk(), u = (unsigned)cell;
+  const unsigned qk = u / nk, qj = qk / nj;
+  const int i = m.b.i0 + (int)qj, j = m.b.j0 + (int)(qk - qj * nj), k = m.b.k0 + (int)(u - qk * nk);
   const int64_t x = g.at(i, j, k);
   T *E = g.F[m.c];
   const int64_t le = m.eofs + cell;
@@ -865,8 +869,10 @@ __global__ void k_sibc_e(Grid<T> g, const SibcSurf *surfs, int nsurf, const Sibc
   const SibcSurf &sf = surfs[s];
   const SibcModelDev &m = models[sf.model];
   int64_t f = t - sf.first;
-  int64_t nj = sf.g.nj(), nk = sf.g.nk();
-  int i = sf.g.i0 + (int)(f / (nj * nk)), j = sf.g.j0 + (int)((f / nk) % nj), k = sf.g.k0 + (int)(f % nk);
+  // A surface holds fewer than 2^31 faces (checked at set-up): 32-bit decode.
+  const unsigned nj = (unsigned)sf.g.nj(), nk = (unsigned)sf.g.nk(), u = (unsigned)f;
+  const unsigned qk = u / nk, qj = qk / nj;
+  int i = sf.g.i0 + (int)qj, j = sf.g.j0 + (int)(qk - qj * nj), k = sf.g.k0 + (int)(u - qk * nk);
   const uint8_t *A = adjA + 4 * t, *B = adjB + 4 * t;
   T *Ex = g.F[EX], *Ey = g.F[EY], *Ez = g.F[EZ];
   const T *Hx = g.F[HX], *Hy = g.F[HY], *Hz = g.F[HZ];
