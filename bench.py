@@ -637,7 +637,9 @@ def enclosure_workload(args, dist=None, cpu=False):
 def batch_workload(args, dist=None):
     """Many independent meshes of uneven size (seeded PEC/dielectric slabs,
     6-cell UPML, a hard or soft dipole), FP32, solved together (solve_batch:
-    engines created one after another, then all stepped side by side, one
+    engines created one after another, then stepped as one group -- one
+    sweep launch per half step over every mesh's tiles, march depth chosen
+    by the autotuner -- or, with --batch-mode streams, side by side on one
     stream per engine), against the plain FP64 path solving them one after
     another.  Solves/s counts create + steps + observer read-back.  The FP64
     path's solves/s is measured on a sample of the meshes (every
@@ -661,23 +663,47 @@ def batch_workload(args, dist=None):
         vb.GpuRun(meshes[0], prec).run(min(64, meshes[0].num_steps)).close()
     torch.cuda.synchronize()
 
+    # The grouped path's tile tuning, chosen by timing a sample of the
+    # meshes (autotune.tune; cached per device and size mix).  It runs before
+    # the timed batch and is reported apart.
+    tuning, tune_rec = None, None
+    if args.batch_mode in ("grouped", "both"):
+        from vulture_b200 import autotune
+
+        tuning, tune_rec = autotune.tune(meshes, "fp32", use_cache=False)
+        torch.cuda.synchronize()
+
     # End to end: engines created one after another, then stepped together
     # (solve_batch), then every solve's observers read back.
-    if dist:
-        dist.barrier()
-    with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        runs = solve_batch(meshes, "fp32")
+    def timed_batch(grouped):
+        if dist:
+            dist.barrier()
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            runs = solve_batch(meshes, "fp32", grouped=grouped, tuning=tuning if grouped else None)
+            for r in runs:
+                r.td()
+                r.dft()
+            wall = time.perf_counter() - t0
+        create = max(r.batch_started for r in runs)
+        step = max(r.batch_finished for r in runs) - create
+        rep = runs[0].batch_report
+        if rep is not None:
+            # The report counts every kernel of the call, per-engine block-end work included.
+            n_launch = rep["launches"]
+        else:
+            n_launch = sum(int(r.stats().kernel_launches) for r in runs)
+        nb = sum(_sweep_bytes(r, "fp32") * r.mesh.num_steps for r in runs)
         for r in runs:
-            r.td()
-            r.dft()
-        wall32 = time.perf_counter() - t0
-    create_s = max(r.batch_started for r in runs)
-    step_s = max(r.batch_finished for r in runs) - create_s
-    launches = sum(int(r.stats().kernel_launches) for r in runs)
-    nbytes = sum(_sweep_bytes(r, "fp32") * r.mesh.num_steps for r in runs)
-    for r in runs:
-        r.close()
+            r.close()
+        return {"wall": wall, "create": create, "step": step, "launches": n_launch, "bytes": nb, "report": rep,
+                "clk": clk}
+
+    modes = {"grouped": [True], "streams": [False], "both": [False, True]}[args.batch_mode]
+    legs = {g: timed_batch(g) for g in modes}
+    main = legs[modes[0]]
+    wall32, create_s, step_s, launches, nbytes, clk = (main["wall"], main["create"], main["step"], main["launches"],
+                                                       main["bytes"], main["clk"])
     # The plain FP64 path: one solve after another, each created, run to its
     # end and read back.
     stride = max(1, len(meshes) // max(1, args.batch_fp64_sample))
@@ -708,8 +734,10 @@ def batch_workload(args, dist=None):
         "config": {"workload": f"{len(meshes)} meshes, per-axis 32-160 cells, 6-cell UPML, PEC/dielectric "
                                f"slabs, dipole; {args.batch_steps[0]}-{args.batch_steps[1]} steps each",
                    "cell_updates": cell_updates,
-                   "batch": "solve_batch: engines created one after another, then vgpu_run_batch, one stream "
-                            "per engine"},
+                   "batch": ("solve_batch: engines created one after another, then vgpu_run_grouped (one sweep "
+                             "launch per half step over every mesh's tiles, autotuned march depth)"
+                             if modes[0] else "solve_batch: engines created one after another, then "
+                             "vgpu_run_batch, one stream per engine")},
         "wall_s": wall32, "create_s": create_s, "step_s": step_s,
         "mcell_updates_per_s_stepping": step_mcell,
         "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
@@ -723,6 +751,23 @@ def batch_workload(args, dist=None):
                         "what": "plain FP64 path, one solve after another (create, run, read back), on every "
                                 f"{stride}-th mesh; whole-batch time = sample mean x {len(meshes)}"},
         "speedup_vs_fp64_sequential": sps32 / sps64, "target_speedup": 3.0,
+        "grouped": (legs[True] and {"solves_per_s": solves / legs[True]["wall"] if world == 1 else None,
+                                    "wall_s": legs[True]["wall"], "step_s": legs[True]["step"],
+                                    "mcell_updates_per_s_stepping": cell_updates / legs[True]["step"] / 1e6,
+                                    "gpu_launches": legs[True]["launches"],
+                                    **{k: legs[True]["report"][k] for k in ("grouped", "rebuilds", "tiles",
+                                                                            "group_ms")},
+                                    "what": "the same batch through vgpu_run_grouped: one sweep launch per half "
+                                            "step over every mesh's tiles, march depth and chunk autotuned"})
+                   if True in legs else None,
+        "tuning": tune_rec and {"march_depth": tune_rec["depth"], "blocks_per_sm": tune_rec["blocks_per_sm"],
+                                "group_chunk": tune_rec["chunk"],
+                                "tune_s": tune_rec["tune_s"], "sample_meshes": tune_rec["sample"],
+                                "steps": tune_rec["steps"],
+                                "trials": [{k: round(t[k], 1) if isinstance(t[k], float) else t[k]
+                                            for k in ("depth", "blocks_per_sm", "chunk", "mcell_per_s")}
+                                           for t in tune_rec["trials"]],
+                                "what": "chosen before the timed batch by timing a sample of the meshes grouped"},
         "gpu_launches": launches, "clocks": clk.summary()}
 
 
@@ -834,6 +879,9 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, nargs=2, default=[2000, 8000])
     ap.add_argument("--batch-fp64-sample", type=int, default=32)
+    ap.add_argument("--batch-mode", default="both", choices=["grouped", "streams", "both"],
+                    help="streams: vgpu_run_batch, one stream per engine; grouped: vgpu_run_grouped (autotuned "
+                         "tiles); both: the two, streams (the faster) as the value and grouped beside it")
     ap.add_argument("--serve-count", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=6.0)
     ap.add_argument("--serve-nmax", type=int, default=256)

@@ -324,6 +324,41 @@ int vgpu_synchronize(vgpu_engine *engine);
  * work is still waited for, and the first error is returned. */
 int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint64_t *steps);
 
+/* Grouped stepping: vgpu_run_batch's contract, with the engines that allow
+ * it stepped as one group per precision.  Each half step of a group is one
+ * sweep launch (per sweep kernel) over the tiles of every member mesh, and
+ * one launch each for all members' observer samples, E sources and H
+ * sources, replayed from captured step graphs; a member leaves the group
+ * when its steps are done (members are ordered by steps left, so a member
+ * leaves by shortening the launches' lists).  An engine joins its precision's group when
+ * vgpu_groupable says so, it sits at a 64-step boundary and it is on the
+ * first engine's device; the others are stepped as vgpu_run_batch steps
+ * them, beside the groups.  Every engine's results are the ones vgpu_run
+ * gives it alone.  `report` (may be NULL) receives the call's counts. */
+typedef struct {
+  uint64_t launches;   /* kernels the call launched, grouped and per engine */
+  int32_t grouped;     /* engines stepped in groups */
+  int32_t rebuilds;    /* changes of a group's membership (members finishing) */
+  int64_t tiles;       /* sweep tiles (E + H) of the groups as they started */
+  double group_ms;     /* device time of the longest group's work */
+} vgpu_group_report;
+int vgpu_run_grouped(vgpu_engine *const *engines, int32_t n, const uint64_t *steps, vgpu_group_report *report);
+
+/* 1 if the engine can step in a group: its steps hold only the sweeps,
+ * point sources and point observers (no Mur, Debye, SIBC, plane wave,
+ * ghost layer or binary observer), and its coefficients are indexed with at
+ * most 64 distinct tuples; 0 if not; a negative status on error. */
+int vgpu_groupable(const vgpu_engine *engine);
+
+/* Sweep tuning for the engines the calling thread creates afterwards and
+ * the groups it runs: march_depth planes per tile (1..32; 0 restores the
+ * built-in rule of about 16 tiles per SM), at most blocks_per_sm resident
+ * sweep blocks per SM (0: as many as fit) and group_chunk, the tiles a
+ * grouped sweep block takes from its launch's counter at a time (1..4096;
+ * 0: 4).  Results do not depend on it; vulture_b200/autotune.py chooses it
+ * by timing. */
+int vgpu_set_sweep_tuning(int32_t march_depth, int32_t blocks_per_sm, int32_t group_chunk);
+
 /* Copy time-domain samples to the host: out[(s*num_td + p)*6 + c] for the
  * first `steps` steps of the output window. */
 int vgpu_read_td(vgpu_engine *engine, double *out, uint64_t steps);

@@ -52,3 +52,28 @@ def test_synthetic_meshes_are_tiled_exactly_once(name):
     for precision in ("fp32", "fp64"):
         bad, ntiles = check(m, precision)
         assert ntiles > 0 and bad == 0, f"{name} {precision}: {bad} violations"
+
+
+@pytest.mark.parametrize("depth", [1, 2, 3, 7, 16, 32])
+def test_tuned_march_depths_tile_exactly_once(depth):
+    """vgpu_set_sweep_tuning's march depth changes the tiles, never the
+    points they claim."""
+    names = ["graded_upml_small", "batch_mesh_0", "serving_request_1"]
+    meshes = [vb.Mesh(stage_text(synthetic()[n], f"{n}.mesh")) for n in names]
+    base = [check(m, "fp32")[1] for m in meshes]
+    vb.set_sweep_tuning(depth, 0, 0)
+    try:
+        for name, m, nb in zip(names, meshes, base):
+            for precision in ("fp32", "fp64"):
+                bad, ntiles = check(m, precision)
+                assert ntiles > 0 and bad == 0, f"{name} {precision} depth {depth}: {bad} violations"
+            if depth == 1:
+                assert check(m, "fp32")[1] > nb
+    finally:
+        vb.set_sweep_tuning(0, 0, 0)
+
+
+def test_sweep_tuning_rejects_out_of_range_values():
+    for args in [(-1, 0, 0), (33, 0, 0), (4, -1, 0), (4, 0, -1), (4, 0, 4097)]:
+        with pytest.raises(N.NativeError):
+            vb.set_sweep_tuning(*args)

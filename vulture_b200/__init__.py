@@ -13,6 +13,6 @@ import os as _os
 # created its CUDA context.
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
-from .solver import GpuRun, Mesh, run_batch, run_mesh  # noqa: E402,F401
+from .solver import GpuRun, Mesh, run_batch, run_grouped, run_mesh, set_sweep_tuning  # noqa: E402,F401
 
-__all__ = ["Mesh", "GpuRun", "run_batch", "run_mesh"]
+__all__ = ["Mesh", "GpuRun", "run_batch", "run_grouped", "run_mesh", "set_sweep_tuning"]

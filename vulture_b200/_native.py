@@ -31,6 +31,11 @@ class VgpuStats(C.Structure):
                 ("merged_parts", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class VgpuGroupReport(C.Structure):
+    _fields_ = [("launches", C.c_uint64), ("grouped", C.c_int32), ("rebuilds", C.c_int32), ("tiles", C.c_int64),
+                ("group_ms", C.c_double)]
+
+
 # void sink(void *user, uint64_t first_row, uint32_t num_rows, int64_t num_points, const float *rows)
 BIN_SINK = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_uint32, C.c_int64, C.POINTER(C.c_float))
 
@@ -93,6 +98,10 @@ def lib() -> C.CDLL:
         "vgpu_synchronize": (C.c_int, [P]),
         "vgpu_run_batch": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(C.c_uint64)]),
         "vgpu_set_sweep_wait_limit": (C.c_int, [C.c_int64]),
+        "vgpu_run_grouped": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(C.c_uint64),
+                                       C.POINTER(VgpuGroupReport)]),
+        "vgpu_groupable": (C.c_int, [P]),
+        "vgpu_set_sweep_tuning": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
     }
@@ -123,7 +132,8 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vgpu_set_bin_sink", "vgpu_dft_accumulate_static", "vhost_num_bin", "vhost_bin_begin", "vhost_bin_sink",
            "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
            "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device",
-           "vgpu_check_sweep_plan", "vgpu_set_sweep_wait_limit"]
+           "vgpu_check_sweep_plan", "vgpu_set_sweep_wait_limit", "vgpu_run_grouped", "vgpu_groupable",
+           "vgpu_set_sweep_tuning"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3
 # Other parts of a step and the 64-step DFT fold, for vgpu_time_kernel.

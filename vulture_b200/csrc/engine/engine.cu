@@ -403,10 +403,18 @@ struct SweepPlan {
   int wn = 0;                         // width of the narrow auxiliary boxes (0: unused)
 };
 
-static SweepPlan plan_sweep(const Box &ub, const RegionSet &rs, bool es, int halo, int nsm)
+// Sweep tuning for the engines a thread creates and the groups it runs
+// (vgpu_set_sweep_tuning): planes per tile (0: the size rule below), a cap
+// on resident blocks per SM (0: as many as fit) and the tiles a grouped
+// sweep block takes at a time (0: 4).
+static thread_local int g_tune_depth = 0, g_tune_blocks = 0, g_tune_chunk = 0;
+
+static SweepPlan plan_sweep(const Box &ub, const RegionSet &rs, bool es, int halo, int nsm, int depth = 0)
 {
   SweepPlan pl;
+  // Planes per tile: about 16 tiles per SM over the update box, 4 to 32.
   auto run_len = [&](int64_t cells) {
+    if (depth > 0) return std::min(depth, kSweepMaxPlanes);
     int64_t t = cells / (256LL * nsm * 16);
     return (int)std::max<int64_t>(4, std::min<int64_t>(kSweepMaxPlanes, t));
   };
@@ -542,6 +550,7 @@ struct Engine : EngineBase {
   // full-volume UPML state.
   struct SweepLaunch {
     SweepTile *tiles = nullptr;
+    std::vector<SweepTile> host;   // the same tiles, for grouped launches
     void *headers = nullptr;     // SweepHeader<T, PML>[ntiles]
     int ntiles = 0, grid = 0;
     uint32_t smem = 0;
@@ -1402,6 +1411,7 @@ struct Engine : EngineBase {
       if (t.i1 - t.i0 + 1 > kSweepMaxPlanes || t.k0 % kSweepKW)
         return set_err(VGPU_EINVAL, "sweep tile of %d planes at k0=%d", t.i1 - t.i0 + 1, t.k0);
     if (upload(&L.tiles, tiles.data(), tiles.size())) return VGPU_ENOMEM;
+    L.host = tiles;
     if (int rc = build_headers<ES, PML>(L, tiles)) return rc;
     L.smem = SweepLayout<T, ES, PML>::smem_bytes(compressed);
     auto kern = k_sweep_tma<T, ES, PML>;
@@ -1413,6 +1423,7 @@ struct Engine : EngineBase {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSweepThreads, L.smem));
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
     if (per_sm < 1) return set_err(VGPU_ECUDA, "sweep kernel does not fit on an SM (%u bytes of shared memory)", L.smem);
+    if (g_tune_blocks > 0) per_sm = std::min(per_sm, g_tune_blocks);
     L.grid = std::min(L.ntiles, per_sm * nsm);
     // Points each launch updates, for throughput accounting.
     const Box *bb = ES ? be : bh;
@@ -1466,7 +1477,7 @@ struct Engine : EngineBase {
     const int halo = 16 / (int)sizeof(T);
     const RegionSet rs = regions_of(p);
     for (int es = 0; es < 2; es++) {
-      SweepPlan pl = plan_sweep(es ? ube : ubh, rs, es != 0, halo, nsm);
+      SweepPlan pl = plan_sweep(es ? ube : ubh, rs, es != 0, halo, nsm, g_tune_depth);
       (es ? maps_e : maps_h).wn = pl.wn;
       SweepLaunch *L = es ? sw_e : sw_h;
       const bool comp = (es ? cie : cih).idx != nullptr;
@@ -1969,7 +1980,16 @@ struct Engine : EngineBase {
       need_sample = false;
     }
     if (int rc = launch_graphs(m)) return rc;
-    step += m;
+    if (int rc = after_block(n0, m, q)) return rc;
+    *queued = m;
+    return 0;
+  }
+
+  // The work that follows a block of m steps from step n0 (the block's
+  // steps are queued on s): binary rows, the DFT fold and the energy check.
+  int after_block(uint64_t n0, uint64_t m, int q)
+  {
+    step = n0 + m;
     // Output rows produced in this block.
     const uint64_t lo = std::max<uint64_t>(n0, p.out_start), hi = std::min<uint64_t>(step - 1, p.out_stop);
     if (p.num_bin > 0 && bin_sink && hi >= lo && lo <= p.out_stop) {
@@ -1983,11 +2003,32 @@ struct Engine : EngineBase {
     // early.
     if (p.num_fd && (step % kChunk == 0 || step == p.num_steps))
       if (int rc = fold_pending()) return rc;
-    (void)hi;
     if (step % kChunk == 0 || step == p.num_steps)
       if (int rc = queue_energy()) return rc;
-    *queued = m;
     return 0;
+  }
+
+  // Whether the engine can step in a group (k_sweep_tma<..., GROUP>,
+  // k_group_side): its steps hold only sweeps, point sources and point
+  // observers, its coefficients are indexed with at most kGroupTab tuples,
+  // and each half step's tiles belong to one sweep kernel.
+  bool groupable() const
+  {
+    if (!cie.idx || !cih.idx || cie.ntab > kGroupTab || cih.ntab > kGroupTab) return false;
+    if (mve.nitems || mvh.nitems || n_debye || nsibc || !pws.empty() || ghost_e || ghost_h || p.num_bin > 0)
+      return false;
+    if (merge_e || merge_obs) return false;
+    for (const SweepLaunch *L : { sw_e, sw_h })
+      if (L[0].ntiles && L[1].ntiles) return false;
+    return true;
+  }
+
+  // The sweep kernel class of a half step's tiles: 0 the bulk kernel, 1
+  // the UPML kernel, -1 none.
+  int sweep_class(bool es) const
+  {
+    const SweepLaunch *L = es ? sw_e : sw_h;
+    return L[1].ntiles ? 1 : L[0].ntiles ? 0 : -1;
   }
 
   // Fold every staged output row of the steps run so far that is not yet in
@@ -2248,6 +2289,440 @@ struct Engine : EngineBase {
   }
 };
 
+// ---- grouped stepping ----------------------------------------------------
+//
+// Many engines of one precision stepped together (the batched form of
+// src/simulation.c:136-231's loop): per half step one launch of the grouped
+// sweep kernel per sweep class over every member's tiles, and one
+// k_group_side launch each for the members' samples, E sources and H
+// sources -- a step of the whole group is at most seven launches however
+// many meshes it holds -- replayed from captured graphs of 16, 8, 4, 2 and 1
+// steps.  Members are ordered by steps left, most first, and every list
+// (tiles, side items, step counters) follows that order; members finish from
+// the end of the order, so the group of the first R members is a prefix of
+// each list and a finished member leaves by shortening the launches (new
+// graphs), with nothing copied.  The sweep blocks take chunks of tiles from
+// a counter per launch (zeroed at each graph's start), so a launch ends
+// evenly.  Every member's kernels do what its own step graph does, in the
+// same order, on its own arrays, so its results are those of vgpu_run
+// alone.
+
+struct GroupBase {
+  virtual ~GroupBase() {}
+  virtual bool busy() const = 0;
+  virtual int issue_block() = 0;
+  virtual int finish() = 0;
+  uint64_t launches = 0;
+  int rebuilds = 0, members_at_start = 0;
+  int64_t tiles_at_start = 0;
+  double ms = 0;
+};
+
+template <typename T>
+struct Group : GroupBase {
+  struct Member {
+    Engine<T> *e;
+    uint64_t left;
+  };
+  // The launches of the first R members, as graphs.
+  struct View {
+    int R = 0;
+    int grid[2][2] = {}, ntiles[2][2] = {};
+    cudaGraphExec_t graphs[5] = {};
+    uint64_t per_step = 0;        // launches of one step
+    cudaEvent_t done = nullptr;   // after this view's last launch
+  };
+  std::vector<Member> members;   // by steps left, most first; the first R are active
+  int R = 0;
+  DevAlloc da;
+  // Device lists, in member order, and the prefix counts per member count.
+  GroupMesh<T> *meshes[2][2] = {};   // [E, H][sweep class]
+  GroupTile *tiles[2][2] = {};
+  std::vector<int> tiles_upto[2][2];   // tiles of the first r members, r = 0..n
+  int *counters = nullptr;             // one per sweep launch of a graph
+  int chunk = 4;                       // tiles a sweep block takes at a time
+  GroupSide<T> *side[3] = {};        // samples, E sources, H sources
+  std::vector<int> side_upto[3], blk_upto[3];
+  uint64_t **steps = nullptr;
+  char *host = nullptr;   // pinned image of the lists
+  View *cur = nullptr;
+  std::vector<View *> retired;
+  cudaStream_t s = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int *d_err = nullptr;
+  int nsm = 148;
+  int per_sm[2][2] = {};
+  std::vector<Engine<T> *> all;   // every member the group started with
+
+  ~Group() override
+  {
+    if (s) cudaStreamSynchronize(s);
+    if (cur) release(cur);
+    for (View *v : retired) release(v);
+    if (host) cudaFreeHost(host);
+    da.free_all();
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  bool busy() const override { return R > 0; }
+
+  template <bool ES, bool PML>
+  int kernel_setup(int h, int c)
+  {
+    auto kern = k_sweep_tma<T, ES, PML, true>;
+    const uint32_t smem = SweepLayout<T, ES, PML>::smem_bytes(true);
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int n = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kSweepThreads, smem));
+    if (n < 1) return set_err(VGPU_ECUDA, "grouped sweep kernel does not fit on an SM (%u bytes of shared memory)", smem);
+    if (g_tune_blocks > 0) n = std::min(n, g_tune_blocks);
+    per_sm[h][c] = n;
+    return 0;
+  }
+
+  void release(View *v)
+  {
+    for (auto &g : v->graphs)
+      if (g) cudaGraphExecDestroy(g);
+    if (v->done) cudaEventDestroy(v->done);
+    delete v;
+  }
+
+  // Streams, flags and the lists; the members' earlier work is finished
+  // first (collect synchronised them).
+  int start()
+  {
+    std::stable_sort(members.begin(), members.end(), [](const Member &a, const Member &b) { return a.left > b.left; });
+    const int n = (int)members.size();
+    R = members_at_start = n;
+    for (Member &mb : members) {
+      all.push_back(mb.e);
+      mb.e->stats.steps = 0;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    if (int rc = kernel_setup<true, false>(0, 0)) return rc;
+    if (int rc = kernel_setup<true, true>(0, 1)) return rc;
+    if (int rc = kernel_setup<false, false>(1, 0)) return rc;
+    if (int rc = kernel_setup<false, true>(1, 1)) return rc;
+    // Layout of one device buffer: each list 256-byte aligned.
+    size_t off = 0;
+    auto place = [&](size_t bytes) {
+      const size_t o = off;
+      off = (off + bytes + 255) / 256 * 256;
+      return o;
+    };
+    const size_t o_err = place(sizeof(int));
+    const size_t o_counters = place(sizeof(int) * kGraphSteps * 4);
+    if (g_tune_chunk > 0) chunk = g_tune_chunk;
+    size_t o_mesh[2][2], o_tiles[2][2];
+    std::vector<int> cls_index[2][2];   // member q's index in its class's mesh array
+    for (int h = 0; h < 2; h++)
+      for (int c = 0; c < 2; c++) {
+        int nm = 0, nt = 0;
+        tiles_upto[h][c].assign(1, 0);
+        cls_index[h][c].assign(n, -1);
+        for (int q = 0; q < n; q++) {
+          Engine<T> *e = members[q].e;
+          if (e->sweep_class(h == 0) == c) {
+            cls_index[h][c][q] = nm++;
+            nt += (h == 0 ? e->sw_e : e->sw_h)[c].ntiles;
+          }
+          tiles_upto[h][c].push_back(nt);
+        }
+        o_mesh[h][c] = place(sizeof(GroupMesh<T>) * (size_t)nm);
+        o_tiles[h][c] = place(sizeof(GroupTile) * (size_t)nt);
+        tiles_at_start += nt;
+      }
+    std::vector<size_t> o_tab(2 * (size_t)n);
+    for (int q = 0; q < n; q++)
+      for (int h = 0; h < 2; h++) {
+        const CoefIndex &ci = h == 0 ? members[q].e->cie : members[q].e->cih;
+        o_tab[2 * q + h] = place((size_t)ci.ntab * (h == 0 ? 6 : 3) * sizeof(T));
+      }
+    std::vector<GroupSide<T>> items[3];
+    std::vector<int> owner[3];
+    for (int k = 0; k < 3; k++) {
+      side_upto[k].assign(1, 0);
+      blk_upto[k].assign(1, 0);
+    }
+    for (int q = 0; q < n; q++) {
+      Engine<T> *e = members[q].e;
+      if (e->p.num_td || e->p.num_fd) {
+        GroupSide<T> it{};
+        it.kind = 0;
+        it.td_pts = e->d_td_pts;
+        it.num_td = e->p.num_td;
+        it.fd_pts = e->d_fd_pts;
+        it.num_fd = e->p.num_fd;
+        it.td_buf = e->d_td;
+        it.fd_stage = e->d_stage;
+        it.out_start = e->p.out_start;
+        it.out_stop = e->out_last();
+        it.tblock = kStageRows;
+        items[0].push_back(it);
+        owner[0].push_back(q);
+      }
+      for (const SrcLaunch &l : e->srcs) {
+        GroupSide<T> it{};
+        it.kind = 1;
+        it.b = l.b;
+        it.c = l.c;
+        it.skind = l.kind;
+        it.soft = (T)l.soft;
+        it.values = (const T *)l.values;
+        const int k = l.c <= EZ ? 1 : 2;
+        items[k].push_back(it);
+        owner[k].push_back(q);
+      }
+    }
+    size_t o_side[3];
+    for (int k = 0; k < 3; k++) o_side[k] = place(sizeof(GroupSide<T>) * items[k].size());
+    const size_t o_grids = place(sizeof(Grid<T>) * (size_t)n);
+    const size_t o_steps = place(sizeof(uint64_t *) * (size_t)n);
+    const size_t total = off;
+    char *dbase = nullptr;
+    if (da.alloc(&dbase, total)) return VGPU_ENOMEM;
+    CK(cudaHostAlloc((void **)&host, total, cudaHostAllocDefault));
+    memset(host, 0, total);
+    d_err = (int *)(dbase + o_err);
+    counters = (int *)(dbase + o_counters);
+    for (int h = 0; h < 2; h++)
+      for (int c = 0; c < 2; c++) {
+        GroupMesh<T> *gm = (GroupMesh<T> *)(host + o_mesh[h][c]);
+        GroupTile *gt = (GroupTile *)(host + o_tiles[h][c]);
+        int nt = 0;
+        for (int q = 0; q < n; q++) {
+          const int r = cls_index[h][c][q];
+          if (r < 0) continue;
+          Engine<T> *e = members[q].e;
+          const auto &L = (h == 0 ? e->sw_e : e->sw_h)[c];
+          GroupMesh<T> &M = gm[r];
+          M.maps = h == 0 ? e->maps_e : e->maps_h;
+          for (int a = 0; a < 3; a++) M.mc.F[a] = e->g.F[(h == 0 ? EX : HX) + a];
+          const PmlFull<T> &pf = h == 0 ? e->pfe : e->pfh;
+          for (int a = 0; a < 6; a++) M.mc.aux[a] = pf.aux[a];
+          M.mc.s0 = e->g.s0;
+          M.mc.s1 = e->g.s1;
+          M.mc.n1 = e->g.n1;
+          M.mc.wn = M.maps.wn;
+          M.headers = L.headers;
+          const CoefIndex &ci = h == 0 ? e->cie : e->cih;
+          M.table = (const T *)(dbase + o_tab[2 * q + h]);
+          M.tab_bytes = (uint32_t)(((size_t)ci.ntab * (h == 0 ? 6 : 3) * sizeof(T) + 15) / 16 * 16);
+          const size_t hb = c ? sizeof(SweepHeader<T, true>) : sizeof(SweepHeader<T, false>);
+          for (int u = 0; u < L.ntiles; u++)
+            gt[nt++] = GroupTile{ L.host[u], r, (const char *)L.headers + hb * (size_t)u, M.table, M.tab_bytes,
+                                  M.mc.wn };
+        }
+        meshes[h][c] = (GroupMesh<T> *)(dbase + o_mesh[h][c]);
+        tiles[h][c] = (GroupTile *)(dbase + o_tiles[h][c]);
+      }
+    Grid<T> *grids_d = (Grid<T> *)(dbase + o_grids);
+    Grid<T> *grids_h = (Grid<T> *)(host + o_grids);
+    uint64_t **steps_h = (uint64_t **)(host + o_steps);
+    for (int q = 0; q < n; q++) {
+      grids_h[q] = members[q].e->g;
+      steps_h[q] = members[q].e->d_step;
+    }
+    for (int k = 0; k < 3; k++) {
+      GroupSide<T> *it = (GroupSide<T> *)(host + o_side[k]);
+      int blk = 0;
+      size_t r = 0;
+      for (int q = 0; q < n; q++) {
+        for (; r < items[k].size() && owner[k][r] == q; r++) {
+          GroupSide<T> x = items[k][r];
+          x.g = grids_d + q;
+          x.step = members[q].e->d_step;
+          const int64_t pts = x.kind == 0 ? (int64_t)(x.num_td + x.num_fd) * 6 : x.b.count();
+          x.first_block = blk;
+          blk += (int)Engine<T>::blocks_for(pts, 128);
+          it[r] = x;
+        }
+        side_upto[k].push_back((int)r);
+        blk_upto[k].push_back(blk);
+      }
+      side[k] = (GroupSide<T> *)(dbase + o_side[k]);
+    }
+    steps = (uint64_t **)(dbase + o_steps);
+    CK(cudaMemcpyAsync(dbase, host, total, cudaMemcpyHostToDevice, s));
+    for (int q = 0; q < n; q++)
+      for (int h = 0; h < 2; h++) {
+        const CoefIndex &ci = h == 0 ? members[q].e->cie : members[q].e->cih;
+        CK(cudaMemcpyAsync(dbase + o_tab[2 * q + h], ci.table, (size_t)ci.ntab * (h == 0 ? 6 : 3) * sizeof(T),
+                           cudaMemcpyDeviceToDevice, s));
+      }
+    if (int rc = new_view()) return rc;
+    CK(cudaEventRecord(t0, s));
+    return 0;
+  }
+
+  // Graphs for the first R members (captured on first use); the previous
+  // view is released once its launches have run.
+  int new_view()
+  {
+    if (cur) {
+      CK(cudaEventRecord(cur->done, s));
+      retired.push_back(cur);
+      cur = nullptr;
+      rebuilds++;
+    }
+    for (size_t q = 0; q < retired.size();) {
+      if (cudaEventQuery(retired[q]->done) == cudaSuccess) {
+        release(retired[q]);
+        retired.erase(retired.begin() + (long)q);
+      } else {
+        cudaGetLastError();
+        q++;
+      }
+    }
+    if (!R) return 0;
+    View *v = new View();
+    cur = v;
+    v->R = R;
+    CK(cudaEventCreateWithFlags(&v->done, cudaEventDisableTiming));
+    for (int h = 0; h < 2; h++)
+      for (int c = 0; c < 2; c++) {
+        const int nt = tiles_upto[h][c][R];
+        v->ntiles[h][c] = nt;
+        v->grid[h][c] = (int)std::min<int64_t>((nt + chunk - 1) / chunk, (int64_t)per_sm[h][c] * nsm);
+      }
+    return 0;
+  }
+
+  template <bool ES, bool PML>
+  void launch_sweep(const View &v, int h, int c, int rel)
+  {
+    static const SweepMaps kNoMaps{};
+    k_sweep_tma<T, ES, PML, true><<<v.grid[h][c], kSweepThreads, SweepLayout<T, ES, PML>::smem_bytes(true), s>>>(
+        kNoMaps, Grid<T>{}, nullptr, nullptr, v.ntiles[h][c], PmlFull<T>{}, CoefIndex{}, d_err, meshes[h][c],
+        tiles[h][c], counters + rel * 4 + h * 2 + c, chunk);
+  }
+
+  // One step's launches for the view's members, `rel` steps past their
+  // counters.
+  uint64_t enqueue_step(const View &v, int rel)
+  {
+    const int r = v.R;
+    uint64_t n = 0;
+    auto side_launch = [&](int k) {
+      if (!side_upto[k][r]) return;
+      k_group_side<T><<<blk_upto[k][r], 128, 0, s>>>(side[k], side_upto[k][r], rel);
+      n++;
+    };
+    auto sweep = [&](int h, int c) {
+      if (!v.grid[h][c]) return;
+      if (h == 0 && c == 0) launch_sweep<true, false>(v, 0, 0, rel);
+      if (h == 0 && c == 1) launch_sweep<true, true>(v, 0, 1, rel);
+      if (h == 1 && c == 0) launch_sweep<false, false>(v, 1, 0, rel);
+      if (h == 1 && c == 1) launch_sweep<false, true>(v, 1, 1, rel);
+      n++;
+    };
+    side_launch(0);
+    sweep(0, 0);
+    sweep(0, 1);
+    side_launch(1);
+    sweep(1, 0);
+    sweep(1, 1);
+    side_launch(2);
+    return n;
+  }
+
+  int capture(View &v, int q)
+  {
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int len = kGraphSteps >> q;
+    uint64_t n = 0;
+    // Every sweep launch of the graph takes its tiles from its own counter.
+    cudaMemsetAsync(counters, 0, sizeof(int) * 4 * len, s);
+    for (int rel = 0; rel < len; rel++) n = enqueue_step(v, rel);
+    k_group_advance<<<Engine<T>::blocks_for(v.R, 128), 128, 0, s>>>(steps, v.R, len);
+    v.per_step = n;
+    const cudaError_t ee = cudaStreamEndCapture(s, &gr);
+    if (ee != cudaSuccess) return set_err(VGPU_ECUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ee));
+    const cudaError_t e = cudaGraphInstantiate(&v.graphs[q], gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+      v.graphs[q] = nullptr;
+      return set_err(VGPU_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    return 0;
+  }
+
+  // The next block: up to the next 64-step boundary and no member past its
+  // count; then each member's own block-end work (DFT fold, energy check)
+  // on the group's stream, and a new view when members have finished.
+  int issue_block() override
+  {
+    // Members sit at the same step modulo the block length; the last active
+    // member has the fewest steps left.
+    uint64_t m = std::min<uint64_t>(kChunk - (members[0].e->step % kChunk), members[R - 1].left);
+    const uint64_t block = m;
+    for (int q = 0; q < 5 && m; q++) {
+      const uint64_t len = (uint64_t)(kGraphSteps >> q);
+      while (m >= len) {
+        if (!cur->graphs[q])
+          if (int rc = capture(*cur, q)) return rc;
+        CK(cudaGraphLaunch(cur->graphs[q], s));
+        launches += len * cur->per_step + 1;
+        m -= len;
+      }
+    }
+    for (int q = 0; q < R; q++) {
+      Member &mb = members[q];
+      Engine<T> *e = mb.e;
+      const uint64_t n0 = e->step;
+      mb.left -= block;
+      e->stats.steps += block;
+      const cudaStream_t own = e->s;
+      e->s = s;
+      const uint64_t before = e->stats.kernel_launches;
+      const int rc = e->after_block(n0, block, (int)((n0 / kChunk) & 1));
+      launches += e->stats.kernel_launches - before;
+      e->s = own;
+      if (rc) return rc;
+    }
+    const int r0 = R;
+    while (R > 0 && members[R - 1].left == 0) R--;
+    if (R != r0)
+      if (int rc = new_view()) return rc;
+    return 0;
+  }
+
+  // Wait for the group's work; a pipeline failure is handed to every
+  // member (its later launches skip, and it reports VGPU_ETIMEOUT).
+  int finish() override
+  {
+    if (!s || !d_err) return 0;
+    CK(cudaEventRecord(t1, s));
+    CK(cudaStreamSynchronize(s));
+    float t = 0;
+    if (cudaEventElapsedTime(&t, t0, t1) == cudaSuccess) ms = t;
+    int h = 0;
+    CK(cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    int rc = 0;
+    std::string msg;
+    for (Engine<T> *e : all) {
+      if (h) CK(cudaMemcpy(e->d_err, &h, sizeof(int), cudaMemcpyHostToDevice));
+      e->stats.run_ms = ms;
+      if (int r = e->finish_queued())
+        if (!rc) {
+          rc = r;
+          msg = g_err;
+        }
+    }
+    if (rc) set_err(rc, "%s", msg.c_str());
+    return rc;
+  }
+};
+
 struct vgpu_engine {
   EngineBase *impl;
   int dev;   // the CUDA device the engine was created on
@@ -2359,7 +2834,7 @@ extern "C" int vgpu_check_sweep_plan(const vgpu_problem *p, int32_t precision, i
     Box bb[3];
     for (int c = 0; c < 3; c++) bb[c] = box_from(p->gfilim[(es ? 0 : 3) + c]);
     if (!es) fold_mur_h(*p, bb);
-    const SweepPlan pl = plan_sweep(unite(bb), rs, es != 0, halo, 148);
+    const SweepPlan pl = plan_sweep(unite(bb), rs, es != 0, halo, 148, g_tune_depth);
     std::vector<SweepTile> all(pl.bulk);
     all.insert(all.end(), pl.pml.begin(), pl.pml.end());
     ntiles += (int64_t)all.size();
@@ -2508,6 +2983,124 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
       rc = r;
       msg = g_err;
     }
+  }
+  if (rc) set_err(rc, "%s", msg.c_str());
+  return rc;
+}
+
+extern "C" int vgpu_set_sweep_tuning(int32_t march_depth, int32_t blocks_per_sm, int32_t group_chunk)
+{
+  if (march_depth < 0 || march_depth > kSweepMaxPlanes || blocks_per_sm < 0 || group_chunk < 0 || group_chunk > 4096)
+    return set_err(VGPU_EINVAL, "sweep tuning: march depth 0..%d, blocks per SM >= 0, group chunk 0..4096",
+                   kSweepMaxPlanes);
+  g_tune_depth = march_depth;
+  g_tune_blocks = blocks_per_sm;
+  g_tune_chunk = group_chunk;
+  return 0;
+}
+
+extern "C" int vgpu_groupable(const vgpu_engine *e)
+{
+  if (!e) return set_err(VGPU_EINVAL, "null engine");
+  EngineBase *b = on_dev(e);
+  if (auto *f = dynamic_cast<Engine<float> *>(b)) return f->groupable() ? 1 : 0;
+  if (auto *d = dynamic_cast<Engine<double> *>(b)) return d->groupable() ? 1 : 0;
+  return 0;
+}
+
+// Members of one precision's group: groupable engines on the first engine's
+// device at a 64-step boundary, after their earlier work has finished.
+template <typename T>
+static int collect(Group<T> &G, vgpu_engine *const *engines, int32_t n, const uint64_t *steps, std::vector<char> &taken)
+{
+  for (int32_t i = 0; i < n; i++) {
+    if (!steps[i] || taken[i] || engines[i]->dev != engines[0]->dev) continue;
+    auto *e = dynamic_cast<Engine<T> *>(on_dev(engines[i]));
+    if (!e || !e->groupable() || e->step % kChunk) continue;
+    if (int rc = e->synchronize()) return rc;
+    G.members.push_back({ e, steps[i] });
+    taken[i] = 1;
+  }
+  // One engine alone gains nothing from a group.
+  if (G.members.size() == 1) {
+    for (int32_t i = 0; i < n; i++)
+      if (engines[i]->impl == G.members[0].e) taken[i] = 0;
+    G.members.clear();
+  }
+  return 0;
+}
+
+extern "C" int vgpu_run_grouped(vgpu_engine *const *engines, int32_t n, const uint64_t *steps,
+                                vgpu_group_report *report)
+{
+  if (report) memset(report, 0, sizeof *report);
+  if (n < 0 || (n && (!engines || !steps))) return set_err(VGPU_EINVAL, "invalid batch");
+  for (int32_t i = 0; i < n; i++) {
+    if (!engines[i]) return set_err(VGPU_EINVAL, "null engine %d in batch", (int)i);
+    for (int32_t k = 0; k < i; k++)
+      if (engines[k] == engines[i]) return set_err(VGPU_EINVAL, "engine %d listed twice in batch", (int)i);
+    if (int rc = on_dev(engines[i])->check_steps(steps[i])) return rc;
+  }
+  if (!n) return 0;
+  std::vector<char> taken((size_t)n, 0);
+  Group<float> g32;
+  Group<double> g64;
+  if (int rc = collect(g32, engines, n, steps, taken)) return rc;
+  if (int rc = collect(g64, engines, n, steps, taken)) return rc;
+  GroupBase *groups[2] = { &g32, &g64 };
+  std::vector<uint64_t> left((size_t)n, 0), before((size_t)n, 0);
+  for (int32_t i = 0; i < n; i++)
+    if (!taken[i]) {
+      left[i] = steps[i];
+      before[i] = on_dev(engines[i])->stats.kernel_launches;
+    }
+  // As vgpu_run_batch: on an error nothing more is queued, everything queued
+  // is waited for, and the first error is returned.
+  int rc = 0;
+  std::string msg;
+  auto fail = [&](int r) {
+    if (r && !rc) {
+      rc = r;
+      msg = g_err;
+    }
+  };
+  cudaSetDevice(engines[0]->dev);
+  if (!g32.members.empty()) fail(g32.start());
+  if (!rc && !g64.members.empty()) fail(g64.start());
+  for (bool any = true; any && !rc;) {
+    any = false;
+    for (GroupBase *g : groups)
+      if (!rc && g->busy()) {
+        cudaSetDevice(engines[0]->dev);
+        fail(g->issue_block());
+        any = any || g->busy();
+      }
+    for (int32_t i = 0; i < n && !rc; i++) {
+      if (!left[i]) continue;
+      uint64_t m = 0;
+      int r = on_dev(engines[i])->enqueue(left[i], &m);
+      if (!r && !m) r = set_err(VGPU_EINVAL, "engine %d in batch reached its last step", (int)i);
+      fail(r);
+      left[i] -= m;
+      any = any || left[i] > 0;
+    }
+  }
+  for (GroupBase *g : groups) {
+    cudaSetDevice(engines[0]->dev);
+    fail(g->finish());
+  }
+  uint64_t launches = g32.launches + g64.launches;
+  for (int32_t i = 0; i < n; i++)
+    if (!taken[i]) {
+      fail(on_dev(engines[i])->synchronize());
+      launches += on_dev(engines[i])->stats.kernel_launches - before[i];
+    }
+  if (report) {
+    report->launches = launches;
+    report->grouped = g32.members_at_start + g64.members_at_start;
+    report->rebuilds = g32.rebuilds + g64.rebuilds;
+    report->tiles = g32.tiles_at_start + g64.tiles_at_start;
+    report->group_ms = std::max(g32.ms, g64.ms);
   }
   if (rc) set_err(rc, "%s", msg.c_str());
   return rc;

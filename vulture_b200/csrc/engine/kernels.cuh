@@ -232,19 +232,26 @@ __global__ void k_debye(Grid<T> g, const DebyeItem *items, int nitems, int64_t t
 // Sources (src/source.c:602-753).
 // ---------------------------------------------------------------------------
 
+// Point t of source box b at step n.
 template <typename T>
-__global__ void k_source(Grid<T> g, Box b, int c, int kind, T soft, const T *values, const uint64_t *step_base,
-                         int step_rel)
+__device__ __forceinline__ void source_point(const Grid<T> &g, const Box &b, int c, int kind, T soft,
+                                             const T *values, uint64_t n, int64_t t)
 {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b.count()) return;
   int64_t nj = b.nj(), nk = b.nk();
   int i = b.i0 + (int)(t / (nj * nk)), j = b.j0 + (int)((t / nk) % nj), k = b.k0 + (int)(t % nk);
   const int64_t x = g.at(i, j, k);
-  T v = values[*step_base + step_rel];
+  T v = values[n];
   T *F = g.F[c];
   if (kind == VGPU_SRC_FIELD) F[x] = soft * F[x] + v;
   else F[x] = soft * F[x] - g.coef(c <= EZ ? 3 + c : 6 + c - HX, x) * v;
+}
+
+template <typename T>
+__global__ void k_source(Grid<T> g, Box b, int c, int kind, T soft, const T *values, const uint64_t *step_base,
+                         int step_rel)
+{
+  source_point(g, b, c, kind, soft, values, *step_base + step_rel, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -387,6 +394,58 @@ __global__ void k_observe(Grid<T> g, const int *td_pts, int num_td, const int *f
 {
   observe_point(g, td_pts, num_td, fd_pts, num_fd, td_buf, fd_stage, *step_base + step_rel, out_start, out_stop,
                 tblock, (int)(blockIdx.x * blockDim.x + threadIdx.x));
+}
+
+// ---------------------------------------------------------------------------
+// Side work of a grouped step (many meshes in one launch): each item is one
+// mesh's observer samples or one of its source boxes, with its own step
+// counter; block b works on the item whose block range holds b.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct GroupSide {
+  const Grid<T> *g;        // the mesh's grid (device copy)
+  const uint64_t *step;    // the mesh's step counter
+  int first_block;         // blocks of the items before this one
+  int kind;                // 0: observer samples, 1: a source box
+  // source box
+  Box b;
+  int c, skind;
+  T soft;
+  const T *values;
+  // observers
+  const int *td_pts, *fd_pts;
+  int num_td, num_fd;
+  T *td_buf;
+  double *fd_stage;
+  uint64_t out_start, out_stop;
+  int tblock;
+};
+
+template <typename T>
+__global__ void k_group_side(const GroupSide<T> *__restrict__ items, int nitems, int step_rel)
+{
+  int lo = 0, hi = nitems - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (items[mid].first_block <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const GroupSide<T> &it = items[lo];
+  const int64_t t = (int64_t)(blockIdx.x - it.first_block) * blockDim.x + threadIdx.x;
+  const uint64_t n = *it.step + step_rel;
+  if (it.kind == 0)
+    observe_point(*it.g, it.td_pts, it.num_td, it.fd_pts, it.num_fd, it.td_buf, it.fd_stage, n, it.out_start,
+                  it.out_stop, it.tblock, (int)t);
+  else
+    source_point(*it.g, it.b, it.c, it.skind, it.soft, it.values, n, t);
+}
+
+// Advance the step counters of a group's meshes by nsteps.
+__global__ void k_group_advance(uint64_t *const *steps, int n, int nsteps)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) *steps[t] += nsteps;
 }
 
 // Twiddles cos/sin(omega_f * t_n) for the rows of one DFT block.

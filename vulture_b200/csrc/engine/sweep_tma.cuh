@@ -190,6 +190,65 @@ struct alignas(16) SweepHeader {
 
 __host__ __device__ constexpr uint32_t round128(uint32_t b) { return (b + 127u) / 128u * 128u; }
 
+// ---- grouped sweeps: one launch over the tiles of many meshes ------------
+//
+// A group launch takes a list of tiles drawn from many independent meshes of
+// one precision (the batched form of the solver's propagate() loop).  Each
+// tile names its mesh and its header; the mesh's descriptor in global memory
+// holds its tensor maps, the per-mesh values the compute warps need and its
+// coefficient table.  The producer brings the mesh values and, when the
+// tile's mesh differs from the one last loaded into that buffer, the
+// coefficient table into shared memory with the tile's stage 0.  Blocks
+// take chunks of consecutive list positions from a counter as they go (the
+// next chunk is requested while the current one issues), so the launch ends
+// evenly however uneven its tiles' costs; the list runs mesh by mesh, so
+// the tiles in flight at one time are neighbours in a few meshes (their
+// halo rows meet in L2) and a block changes mesh at most once per chunk.
+// After its last tile the producer hands the compute warps a stage 0 whose
+// header holds no planes, which ends their loop.
+
+constexpr int kGroupTab = 64;   // coefficient tuples a grouped mesh may have
+
+// Per-mesh values the compute warps read, copied into shared memory with a
+// tile's stage 0.
+template <typename T>
+struct alignas(16) GroupMeshCompute {
+  T *F[3];          // the three updated components
+  T *aux[6];        // full-volume UPML auxiliaries (PmlFull)
+  int64_t s0, s1;   // strides of i and j
+  int n1, wn;       // j extent; width of the narrow auxiliary boxes
+  int pad[2];
+};
+
+// One mesh of a group.  Tensor maps in global memory are copied to the
+// device by a stream-ordered copy before the launch; the producer fences
+// them (tensormap proxy acquire, GPU scope) when it moves to the mesh, so
+// its TMA loads read the maps as copied, not a descriptor cached from
+// earlier contents of the same address.
+template <typename T>
+struct alignas(64) GroupMesh {
+  SweepMaps maps;
+  GroupMeshCompute<T> mc;
+  const void *headers;   // SweepHeader<T, PML>[this mesh's tiles]
+  const T *table;        // coefficient tuples, 16-byte aligned
+  uint32_t tab_bytes;    // the table's bytes, a multiple of 16
+  int pad;
+};
+
+struct GroupTile {
+  SweepTile t;
+  int mesh;            // index into the group's GroupMesh array
+  const void *hdr;     // the tile's SweepHeader<T, PML>
+  const void *table;   // the mesh's coefficient tuples (16-byte aligned)
+  uint32_t tab_bytes;  // the table's bytes, a multiple of 16
+  int wn;              // the mesh's narrow auxiliary box width
+};
+
+__device__ __forceinline__ void fence_tensormap(const CUtensorMap *m)
+{
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((uint64_t)m) : "memory");
+}
+
 template <typename T, bool ESWEEP, bool PML>
 struct SweepLayout {
   static constexpr int JH = kSweepJH;
@@ -220,22 +279,30 @@ struct SweepLayout {
   __host__ __device__ static constexpr uint32_t smem_bytes(bool compressed) { return S * stage_bytes(compressed); }
 };
 
-// Block: warps 0..7 compute, warp 8 lane 0 produces.
-template <typename T, bool ESWEEP, bool PML>
+// Block: warps 0..7 compute, warp 8 lane 0 produces.  GROUP: the ntiles
+// tiles gtiles of many meshes (gm), taken `chunk` at a time from *counter
+// (zero at launch); maps, g, tiles, headers, pf and ci are unused.  Every
+// grouped mesh has a coefficient index of at most kGroupTab tuples.
+template <typename T, bool ESWEEP, bool PML, bool GROUP = false>
 __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MIN_BLOCKS)
     k_sweep_tma(const __grid_constant__ SweepMaps maps, Grid<T> g, const SweepTile *__restrict__ tiles,
-                const SweepHeader<T, PML> *__restrict__ headers, int ntiles, PmlFull<T> pf, CoefIndex ci, int *err)
+                const SweepHeader<T, PML> *__restrict__ headers, int ntiles, PmlFull<T> pf, CoefIndex ci, int *err,
+                const GroupMesh<T> *__restrict__ gm = nullptr, const GroupTile *__restrict__ gtiles = nullptr,
+                int *counter = nullptr, int chunk = 1)
 {
   using L = SweepLayout<T, ESWEEP, PML>;
   using Hdr = SweepHeader<T, PML>;
+  using MC = GroupMeshCompute<T>;
   constexpr int S = L::S, W = L::W, HALO = L::HALO, KW = kSweepKW;
+  constexpr int TAB = (GROUP ? kGroupTab : 256) * L::NCOEF;   // one table buffer
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[S], empty[S];
-  __shared__ T tab[256 * L::NCOEF];
+  __shared__ __align__(16) T tab[(GROUP ? 2 : 1) * TAB];
   __shared__ Hdr hdr[2];
+  __shared__ MC mcs[GROUP ? 2 : 1];
   __shared__ int sh_err;
 
-  const bool compressed = ci.idx != nullptr;
+  const bool compressed = GROUP || ci.idx != nullptr;
   const uint32_t stage_b = L::stage_bytes(compressed);
   const int tid = threadIdx.x;
   const int warp = tid / 32, lane = tid % 32;
@@ -249,7 +316,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
     }
     mbar_fence_init();
   }
-  if (compressed) {
+  if (!GROUP && compressed) {
     const T *src = (const T *)ci.table;
     for (int q = tid; q < ci.ntab * L::NCOEF; q += kSweepThreads) tab[q] = src[q];
   }
@@ -260,15 +327,74 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
     // ---- producer ----
     if (lane != 0) return;
     const uint32_t full_tx = L::full_tx(compressed);
-    const uint32_t narrow_tx = full_tx - L::NAUX * L::OWN_B + L::NAUX * (uint32_t)(maps.wn * L::JH * sizeof(T));
     uint32_t gs = 0;
     bool ok = true;
-    int id = blockIdx.x;
-    SweepTile tt = id < ntiles ? tiles[id] : SweepTile{};
-    for (uint32_t m = 0; ok && id < ntiles; m++) {
+    // Solo: positions blockIdx.x, + gridDim.x, ...  GROUP: the current
+    // chunk [.., cend) and the start of the next one, already requested.
+    int id = (int)blockIdx.x, cend = 0, pend = 0;
+    if (GROUP) {
+      id = atomicAdd(counter, chunk);
+      cend = min(id + chunk, ntiles);
+      pend = id < ntiles ? atomicAdd(counter, chunk) : ntiles;
+    }
+    auto next_pos = [&](int cur) {
+      if (!GROUP) return cur + (int)gridDim.x;
+      if (cur + 1 < cend) return cur + 1;
+      const int n0 = pend;
+      cend = min(n0 + chunk, ntiles);
+      pend = n0 < ntiles ? atomicAdd(counter, chunk) : ntiles;
+      return n0;
+    };
+    SweepTile tt{};
+    GroupTile gt{};
+    if (id < ntiles) {
+      if (GROUP) gt = gtiles[id];
+      else tt = tiles[id];
+    }
+    // GROUP: the mesh of the previous tile (its maps fenced), the meshes
+    // whose tables the two table buffers hold, and the last stage of the
+    // previous two tiles (buffer b of the header, mesh values and table is
+    // rewritten only after every compute warp has released the last stage
+    // of the tile that read it).
+    int cur_mesh = -1, tab_mesh0 = -1, tab_mesh1 = -1;
+    uint32_t fenced = 0;   // map sets of cur_mesh fenced: 1 own/oth/idx, 2 aux, 4 auxn
+    int64_t last1 = -1, last2 = -1;
+    uint32_t m = 0;
+    for (; ok && id < ntiles; m++) {
       // The next tile's record loads while this one issues.
-      const int id_next = id + (int)gridDim.x;
-      const SweepTile nt = id_next < ntiles ? tiles[id_next] : SweepTile{};
+      const int id_next = next_pos(id);
+      SweepTile nt{};
+      GroupTile ngt{};
+      if (id_next < ntiles) {
+        if (GROUP) ngt = gtiles[id_next];
+        else nt = tiles[id_next];
+      }
+      if (GROUP) tt = gt.t;
+      const SweepMaps *mp = &maps;
+      if (GROUP) {
+        // Each set of the mesh's maps is fenced before its first use since
+        // the block moved to the mesh.
+        mp = &gm[gt.mesh].maps;
+        if (gt.mesh != cur_mesh) {
+          cur_mesh = gt.mesh;
+          fenced = 0;
+        }
+        const uint32_t need = 1u | (PML && tt.reg[0] >= 0 ? (tt.ax < 0 ? 2u : 4u) : 0u);
+        if (need & ~fenced & 1u) {
+          for (int c = 0; c < 3; c++) {
+            fence_tensormap(&mp->own[c]);
+            fence_tensormap(&mp->oth[c]);
+          }
+          fence_tensormap(&mp->idx);
+        }
+        if (need & ~fenced & 2u)
+          for (int c = 0; c < L::NAUX; c++) fence_tensormap(&mp->aux[c]);
+        if (need & ~fenced & 4u)
+          for (int c = 0; c < L::NAUX; c++) fence_tensormap(&mp->auxn[c]);
+        fenced |= need;
+      }
+      const int wn = GROUP ? gt.wn : maps.wn;
+      const uint32_t narrow_tx = full_tx - L::NAUX * L::OWN_B + L::NAUX * (uint32_t)(wn * L::JH * sizeof(T));
       const int n = tt.i1 - tt.i0 + 1;
       const int xs_o = ESWEEP ? tt.k0 - HALO : tt.k0;
       const int yo = ESWEEP ? tt.j0 - 1 : tt.j0;
@@ -282,34 +408,73 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
         uint64_t *bar = &full[slot];
         const int i = ESWEEP ? tt.i0 - 1 + q : tt.i1 + 1 - q;
         if (q == 0) {
-          mbar_arrive_expect_tx(bar, L::PARTIAL_TX);
-          bulk_load(&hdr[m & 1], headers + id, (uint32_t)sizeof(Hdr), bar);
+          if (GROUP) {
+            const int b = (int)(m & 1);
+            const bool need_tab = (b ? tab_mesh1 : tab_mesh0) != gt.mesh;
+            // The tile two back read buffer b (its mesh values and table) in
+            // every plane: wait until its last stage is released (older
+            // stages are covered by the ring's wait above).
+            if (last2 >= 0 && (uint64_t)last2 + S > gs && !mbar_wait(&empty[last2 % S], (uint32_t)(last2 / S) & 1)) {
+              ok = false;
+              break;
+            }
+            const uint32_t tb = need_tab ? gt.tab_bytes : 0u;
+            mbar_arrive_expect_tx(bar, L::PARTIAL_TX + (uint32_t)sizeof(MC) + tb);
+            bulk_load(&hdr[b], gt.hdr, (uint32_t)sizeof(Hdr), bar);
+            bulk_load(&mcs[b], &gm[gt.mesh].mc, (uint32_t)sizeof(MC), bar);
+            if (need_tab) {
+              bulk_load(tab + b * TAB, gt.table, tb, bar);
+              if (b) tab_mesh1 = gt.mesh;
+              else tab_mesh0 = gt.mesh;
+            }
+          } else {
+            mbar_arrive_expect_tx(bar, L::PARTIAL_TX);
+            bulk_load(&hdr[m & 1], headers + id, (uint32_t)sizeof(Hdr), bar);
+          }
           for (int c = 1; c < 3; c++)
-            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
+            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &mp->oth[c], bar, xs_o, yo, i);
         } else {
           // Tiles of bulk points only (reg[0] < 0) load no auxiliaries.
           const bool has_aux = tt.reg[0] >= 0;
           mbar_arrive_expect_tx(bar, !has_aux ? full_tx - L::NAUX * L::OWN_B : (tt.ax < 0 ? full_tx : narrow_tx));
           for (int c = 0; c < 3; c++)
-            tma_load_3d(st + L::OFF_OWN + c * round128(L::OWN_B), &maps.own[c], bar, tt.k0, tt.j0, i);
+            tma_load_3d(st + L::OFF_OWN + c * round128(L::OWN_B), &mp->own[c], bar, tt.k0, tt.j0, i);
           for (int c = 0; c < 3; c++)
-            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &maps.oth[c], bar, xs_o, yo, i);
+            tma_load_3d(st + L::OFF_OTH + c * round128(L::OTH_B), &mp->oth[c], bar, xs_o, yo, i);
           for (int c = 0; c < (has_aux ? L::NAUX : 0); c++) {
             if (tt.ax < 0)
-              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.aux[c], bar, tt.k0, tt.j0, i);
+              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &mp->aux[c], bar, tt.k0, tt.j0, i);
             else
-              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &maps.auxn[c], bar, tt.ax, tt.j0, i);
+              tma_load_3d(st + L::OFF_AUX + c * round128(L::OWN_B), &mp->auxn[c], bar, tt.ax, tt.j0, i);
           }
           if (compressed)
-            tma_load_3d(st + L::OFF_CF, &maps.idx, bar, tt.k0, tt.j0, i);
+            tma_load_3d(st + L::OFF_CF, &mp->idx, bar, tt.k0, tt.j0, i);
           else
             for (int c = 0; c < L::NCOEF; c++)
-              tma_load_3d(st + L::OFF_CF + c * round128(L::OWN_B), &maps.coef[c], bar, tt.k0, tt.j0, i);
+              tma_load_3d(st + L::OFF_CF + c * round128(L::OWN_B), &mp->coef[c], bar, tt.k0, tt.j0, i);
         }
         gs++;
       }
+      last2 = last1;
+      last1 = (int64_t)gs - 1;
       id = id_next;
-      tt = nt;
+      if (GROUP) gt = ngt;
+      else tt = nt;
+    }
+    // GROUP: a stage 0 whose header holds no planes ends the compute warps'
+    // loop.  Written by this thread into the header buffer, then released
+    // by a plain arrival (the barrier expects one arrival and no bytes).
+    if (GROUP && ok) {
+      const uint32_t slot = gs % S;
+      if ((gs >= S && !mbar_wait(&empty[slot], ((gs / S) - 1) & 1)) ||
+          (last2 >= 0 && (uint64_t)last2 + S > gs && !mbar_wait(&empty[last2 % S], (uint32_t)(last2 / S) & 1))) {
+        ok = false;
+      } else {
+        hdr[m & 1].t.i0 = 1;
+        hdr[m & 1].t.i1 = 0;
+        mbar_arrive(&full[slot]);
+        gs++;
+      }
     }
     if (!ok) atomicCAS(err, 0, 1);
     // No load may still be in flight when the block's last thread leaves.
@@ -320,14 +485,11 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
   // ---- compute warps ----
   const uint32_t full_polls = *(volatile uint32_t *)&g_full_wait_polls;
   const int kl = tid % KW, jl = tid / KW;
-  T *__restrict__ F0 = g.F[ESWEEP ? EX : HX];
-  T *__restrict__ F1 = g.F[ESWEEP ? EY : HY];
-  T *__restrict__ F2 = g.F[ESWEEP ? EZ : HZ];
   const int io = jl * KW + kl;                        // row-wide boxes
   const int ih = (ESWEEP ? jl + 1 : jl) * W + (ESWEEP ? kl + HALO : kl);   // curl boxes
   uint32_t gs = 0;
   for (uint32_t m = 0;; m++) {
-    if ((int)(blockIdx.x + m * gridDim.x) >= ntiles) return;
+    if (!GROUP && (int)(blockIdx.x + m * gridDim.x) >= ntiles) return;
     // Stage 0 of the tile, with its header.
     uint32_t slot = gs % S;
     bool ok = mbar_wait(&full[slot], (gs / S) & 1, full_polls);
@@ -337,14 +499,24 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
     }
     const Hdr &h = hdr[m & 1];
     const SweepTile t = h.t;
+    if (GROUP && t.i1 < t.i0) return;   // the producer's end mark
+    // The tile's mesh: the launch's own (solo) or the one stage 0 brought.
+    const MC &mc = mcs[GROUP ? (m & 1) : 0];
+    T *__restrict__ F0 = GROUP ? mc.F[0] : g.F[ESWEEP ? EX : HX];
+    T *__restrict__ F1 = GROUP ? mc.F[1] : g.F[ESWEEP ? EY : HY];
+    T *__restrict__ F2 = GROUP ? mc.F[2] : g.F[ESWEEP ? EZ : HZ];
+    const int64_t s0 = GROUP ? mc.s0 : g.s0, s1 = GROUP ? mc.s1 : g.s1;
+    const int n1 = GROUP ? mc.n1 : g.n1;
+    const int wn = GROUP ? mc.wn : maps.wn;
+    const T *tabm = tab + (GROUP ? (int)(m & 1) * TAB : 0);
     const int n = t.i1 - t.i0 + 1;
     const int k = t.k0 + kl;
     const int j = t.j0 + jl;
     // UPML auxiliaries: full-width boxes share the row-wide layout.
-    const int ia = t.ax < 0 ? io : jl * maps.wn + (k - t.ax);
-    const int jc = min(j, g.n1 - 1);
-    const int kc = min(k, (int)g.s1 - 1);
-    const int64_t x0 = (int64_t)jc * g.s1 + kc;
+    const int ia = t.ax < 0 ? io : jl * wn + (k - t.ax);
+    const int jc = min(j, n1 - 1);
+    const int kc = min(k, (int)s1 - 1);
+    const int64_t x0 = (int64_t)jc * s1 + kc;
     const uint32_t col = h.row_mask[jl] & h.col_mask[kl];
     const uint32_t pm_l = h.plane_mask[lane];
     const T d1 = h.dy[jl], d2 = h.dz[kl], dx_l = h.dx[lane];
@@ -391,7 +563,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       T cf[L::NCOEF];
       if (compressed) {
         const uint8_t *ix = (const uint8_t *)(sc + L::OFF_CF);
-        const T *cw = tab + L::NCOEF * (int)ix[io];
+        const T *cw = tabm + L::NCOEF * (int)ix[io];
 #pragma unroll
         for (int c = 0; c < L::NCOEF; c++) cf[c] = cw[c];
       } else {
@@ -438,7 +610,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       if (lane == 0) mbar_arrive(&empty[slot]);
       gs++;
 
-      const int64_t x = x0 + (int64_t)i * g.s0;
+      const int64_t x = x0 + (int64_t)i * s0;
       // UPML-region tiles hold no bulk points: the branch is uniform.
       if (!PML || t.bulk) {
         if (ESWEEP) {
@@ -454,6 +626,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       // Bulk-only tiles (reg[0] < 0, the same for the whole block) skip the
       // UPML part, profile shuffles included.
       if (PML && t.reg[0] >= 0) {
+#define AUX(c) (GROUP ? mc.aux[c] : pf.aux[c])
         const T xa = __shfl_sync(0xffffffffu, pa_l, p), xb = __shfl_sync(0xffffffffu, pb_l, p);
         const T xc = __shfl_sync(0xffffffffu, pc_l, p), xd = __shfl_sync(0xffffffffu, pd_l, p);
         if (ESWEEP) {
@@ -461,23 +634,23 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
           // change; E from P's change.  (a, b, c, d) = (ad, bd, ah, ibh).
           if (sel & 8u) {
             const T nPP = cf[0] * ax0 + cf[3] * c0;
-            pf.aux[0][x] = nPP;
+            AUX(0)[x] = nPP;
             const T nP = q1a * ax3 + q1b * (nPP - ax0);
-            pf.aux[3][x] = nP;
+            AUX(3)[x] = nP;
             F0[x] = q2a * v0 + q2b * xd * (nP - xc * ax3);
           }
           if (sel & 16u) {
             const T nPP = cf[1] * ax1 + cf[4] * c1;
-            pf.aux[1][x] = nPP;
+            AUX(1)[x] = nPP;
             const T nP = q2a * ax4 + q2b * (nPP - ax1);
-            pf.aux[4][x] = nP;
+            AUX(4)[x] = nP;
             F1[x] = xa * v1 + xb * q1d * (nP - q1c * ax4);
           }
           if (sel & 32u) {
             const T nPP = cf[2] * ax2 + cf[5] * c2;
-            pf.aux[2][x] = nPP;
+            AUX(2)[x] = nPP;
             const T nP = xa * ax5 + xb * (nPP - ax2);
-            pf.aux[5][x] = nP;
+            AUX(5)[x] = nP;
             F2[x] = q1a * v2 + q1b * q2d * (nP - q2c * ax5);
           }
         } else {
@@ -485,20 +658,21 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
           // change.  (a, b, c, d) = (ah, bh, ad, ibd).
           if (sel & 8u) {
             const T nB = q1a * ax0 + cf[0] * q1b * c0;
-            pf.aux[0][x] = nB;
+            AUX(0)[x] = nB;
             F0[x] = q2a * v0 + q2b * xd * (nB - xc * ax0);
           }
           if (sel & 16u) {
             const T nB = q2a * ax1 + cf[1] * q2b * c1;
-            pf.aux[1][x] = nB;
+            AUX(1)[x] = nB;
             F1[x] = xa * v1 + xb * q1d * (nB - q1c * ax1);
           }
           if (sel & 32u) {
             const T nB = xa * ax2 + cf[2] * xb * c2;
-            pf.aux[2][x] = nB;
+            AUX(2)[x] = nB;
             F2[x] = q1a * v2 + q1b * q2d * (nB - q2c * ax2);
           }
         }
+#undef AUX
       }
     }
   }

@@ -181,6 +181,14 @@ class GpuRun:
     def step(self) -> int:
         return int(N.lib().vgpu_current_step(self._e))
 
+    @property
+    def groupable(self) -> bool:
+        """Whether the engine can step in a group (vgpu_groupable)."""
+        rc = N.lib().vgpu_groupable(self._e)
+        if rc < 0:
+            N.check_gpu(rc)
+        return rc == 1
+
     def enqueue(self, max_steps: int = 64) -> int:
         """Queue up to max_steps more steps (one 64-step block at most) without
         waiting; returns the steps queued, 0 once the problem is done."""
@@ -271,6 +279,30 @@ def run_batch(runs, steps=None):
     st = (C.c_uint64 * n)(*steps)
     N.check_gpu(N.lib().vgpu_run_batch(arr, n, st))
     return runs
+
+
+def run_grouped(runs, steps=None):
+    """Advance several GpuRun engines of one device together with grouped
+    launches (vgpu_run_grouped): the engines that allow it share one sweep
+    launch per half step; steps[i] more steps each (default: to the end of
+    each problem).  Returns the call's report as a dict."""
+    n = len(runs)
+    if steps is None:
+        steps = [r.mesh.num_steps - r.step for r in runs]
+    arr = (C.c_void_p * n)(*[r._e.value for r in runs])
+    st = (C.c_uint64 * n)(*steps)
+    rep = N.VgpuGroupReport()
+    N.check_gpu(N.lib().vgpu_run_grouped(arr, n, st, C.byref(rep)))
+    return {"launches": int(rep.launches), "grouped": int(rep.grouped), "rebuilds": int(rep.rebuilds),
+            "tiles": int(rep.tiles), "group_ms": float(rep.group_ms)}
+
+
+def set_sweep_tuning(march_depth: int = 0, blocks_per_sm: int = 0, group_chunk: int = 0) -> None:
+    """Sweep tiling for engines this thread creates afterwards and groups it
+    runs: planes per tile (0: the built-in rule), a cap on resident sweep
+    blocks per SM (0: none) and the tiles a grouped sweep block takes at a
+    time (0: 4).  Results do not depend on it."""
+    N.check_gpu(N.lib().vgpu_set_sweep_tuning(int(march_depth), int(blocks_per_sm), int(group_chunk)))
 
 
 def run_mesh(mesh_path, out_dir, precision="fp64", full_precision=False):
