@@ -105,6 +105,31 @@ def make_mesh(directory: Path, nt: int, plane: int = None) -> Path:
     return Path(meshgen.write(meshgen.graded_upml(seed=2, **kw), directory / "graded_upml.mesh"))
 
 
+# Untimed steps before a timed region, inside the clock record: 128 (two
+# 64-step blocks, about 20 ms of config 2) bring the GPU out of the idle
+# clocks it drops to while the clock sampler starts, then the W warm-up steps,
+# which also capture the short step graphs the timed steps replay.
+PREHEAT_STEPS = 128
+
+
+def warm_then_time(g, args, dist, local):
+    """PREHEAT_STEPS + W untimed steps, then exactly K timed steps (the
+    engine's run_ms: CUDA events on its stream), with a barrier and a device
+    synchronisation on both sides; returns the clock record."""
+    import torch
+
+    with ClockSampler(local) as clk:
+        g.run(PREHEAT_STEPS + args.warmup)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        g.run(args.steps)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return clk
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during a region."""
 
@@ -363,7 +388,7 @@ def run_gpu_arm(args):
 
     prec = args.precision
     work = Path(tempfile.mkdtemp(prefix=f"vb_bench_{rank}_"))
-    nt = max(WORKLOAD["nt"], args.warmup + args.steps)
+    nt = max(WORKLOAD["nt"], PREHEAT_STEPS + args.warmup + args.steps)
     mesh_path = make_mesh(work, nt)
     old = os.getcwd()
     os.chdir(work)
@@ -372,17 +397,9 @@ def run_gpu_arm(args):
     n_out = m.num_cells
     assert n_out == N_OUT, (n_out, N_OUT)
 
-    # Device-resident timing: W untimed steps, then exactly K timed steps.
+    # Device-resident timing: untimed steps, then exactly K timed steps.
     g = vb.GpuRun(m, prec)
-    g.run(args.warmup)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    with ClockSampler(local) as clk:
-        g.run(args.steps)
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    clk = warm_then_time(g, args, dist, local)
     st = g.stats()
     ms = st.run_ms
     launches = int(st.kernel_launches)
@@ -483,6 +500,7 @@ def run_gpu_arm(args):
         out = {
             "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "untimed_steps_before": PREHEAT_STEPS + args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": prec,
             "data": "synthetic", "config": dict(CONFIG, precision=prec),
             "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec],
@@ -555,13 +573,7 @@ def enclosure_workload(args, dist=None, cpu=False):
     n_out = m.num_cells
     prec = "fp32"
     g = vb.GpuRun(m, prec)
-    g.run(args.warmup)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    with ClockSampler(local) as clk:
-        g.run(args.steps)
-        torch.cuda.synchronize()
+    clk = warm_then_time(g, args, dist, local)
     st = g.stats()
     ms = max_over_ranks(st.run_ms, dist)
     value = replica_throughput(n_out, args.steps, ms, world)
@@ -599,6 +611,7 @@ def enclosure_workload(args, dist=None, cpu=False):
     out = {
         "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "dtype": prec,
+        "untimed_steps_before": PREHEAT_STEPS + args.warmup,
         "config": {"workload": "shielded enclosure 400x300x250 graded, Mur, SIBC box with aperture, 4 PEC wires, "
                                "TFSF, 128x128 + 8 FD points x 500 frequencies, 20000 steps",
                    "n_out_cells": n_out, "precision": prec, "dft": "fp64"},
