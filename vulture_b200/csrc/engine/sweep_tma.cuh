@@ -297,6 +297,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
   constexpr int TAB = (GROUP ? kGroupTab : 256) * L::NCOEF;   // one table buffer
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[S], empty[S];
+  __shared__ uint64_t tdone[2];   // GROUP: every compute warp has finished a tile that used buffer b
   __shared__ __align__(16) T tab[(GROUP ? 2 : 1) * TAB];
   __shared__ Hdr hdr[2];
   __shared__ MC mcs[GROUP ? 2 : 1];
@@ -314,6 +315,8 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 8);
     }
+    if (GROUP)
+      for (int b = 0; b < 2; b++) mbar_init(&tdone[b], 8);
     mbar_fence_init();
   }
   if (!GROUP && compressed) {
@@ -351,14 +354,13 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
       if (GROUP) gt = gtiles[id];
       else tt = tiles[id];
     }
-    // GROUP: the mesh of the previous tile (its maps fenced), the meshes
-    // whose tables the two table buffers hold, and the last stage of the
-    // previous two tiles (buffer b of the header, mesh values and table is
-    // rewritten only after every compute warp has released the last stage
-    // of the tile that read it).
+    // GROUP: the mesh of the previous tile (its maps fenced) and the meshes
+    // whose tables the two table buffers hold.  Buffer b (m & 1) of the
+    // header, mesh values and table is rewritten for tile m only once every
+    // compute warp has finished tile m - 2 (tdone[b]): a warp reads the mesh
+    // values while it stores, after it has released the tile's last stage.
     int cur_mesh = -1, tab_mesh0 = -1, tab_mesh1 = -1;
     uint32_t fenced = 0;   // map sets of cur_mesh fenced: 1 own/oth/idx, 2 aux, 4 auxn
-    int64_t last1 = -1, last2 = -1;
     uint32_t m = 0;
     for (; ok && id < ntiles; m++) {
       // The next tile's record loads while this one issues.
@@ -411,10 +413,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
           if (GROUP) {
             const int b = (int)(m & 1);
             const bool need_tab = (b ? tab_mesh1 : tab_mesh0) != gt.mesh;
-            // The tile two back read buffer b (its mesh values and table) in
-            // every plane: wait until its last stage is released (older
-            // stages are covered by the ring's wait above).
-            if (last2 >= 0 && (uint64_t)last2 + S > gs && !mbar_wait(&empty[last2 % S], (uint32_t)(last2 / S) & 1)) {
+            if (m >= 2 && !mbar_wait(&tdone[b], ((m >> 1) - 1) & 1)) {
               ok = false;
               break;
             }
@@ -455,8 +454,6 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
         }
         gs++;
       }
-      last2 = last1;
-      last1 = (int64_t)gs - 1;
       id = id_next;
       if (GROUP) gt = ngt;
       else tt = nt;
@@ -467,7 +464,7 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
     if (GROUP && ok) {
       const uint32_t slot = gs % S;
       if ((gs >= S && !mbar_wait(&empty[slot], ((gs / S) - 1) & 1)) ||
-          (last2 >= 0 && (uint64_t)last2 + S > gs && !mbar_wait(&empty[last2 % S], (uint32_t)(last2 / S) & 1))) {
+          (m >= 2 && !mbar_wait(&tdone[m & 1], ((m >> 1) - 1) & 1))) {
         ok = false;
       } else {
         hdr[m & 1].t.i0 = 1;
@@ -674,6 +671,11 @@ __global__ void __launch_bounds__(kSweepThreads, SweepLayout<T, ESWEEP, PML>::MI
         }
 #undef AUX
       }
+    }
+    if (GROUP) {
+      // Every read of buffer m & 1 by this warp is done.
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tdone[m & 1]);
     }
   }
 }
