@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
@@ -119,20 +121,109 @@ static int host_threads()
   return std::max(1, std::min(32, hw / busy));
 }
 
+// Host threads for set-up and read-back work, started once and kept: a
+// thread started per parallel section costs tens of microseconds, more than
+// the section's work on a small mesh, and a creation or read-back has tens
+// of sections.  run(n, fn) calls fn(0 .. n-1) on the pool and the calling
+// thread and returns when all have returned.  One section runs at a time
+// (creations on several threads take turns with their sections); a section
+// started from inside a section runs on the calling thread alone.
+class HostPool {
+ public:
+  static HostPool &get()
+  {
+    static HostPool *p = new HostPool();   // never destroyed: its threads live until exit
+    return *p;
+  }
+  int size() const { return (int)threads_.size() + 1; }
+  template <typename F>
+  void run(int n, F &&fn)
+  {
+    if (n <= 0) return;
+    if (n == 1 || in_section()) {
+      for (int w = 0; w < n; w++) fn(w);
+      return;
+    }
+    std::lock_guard<std::mutex> section(run_mu_);
+    std::function<void(int)> job = fn;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &job;
+      n_ = n;
+      next_ = 0;
+      left_ = n;
+      gen_++;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return left_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  HostPool()
+  {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    for (int q = 1; q < std::min(hw, 32); q++) threads_.emplace_back([this] { loop(); });
+    for (auto &t : threads_) t.detach();
+  }
+  static bool &in_section()
+  {
+    static thread_local bool f = false;
+    return f;
+  }
+  // Take items of the current section until none is left.
+  void work()
+  {
+    in_section() = true;
+    for (;;) {
+      int w;
+      const std::function<void(int)> *job;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!job_ || next_ >= n_) break;
+        w = next_++;
+        job = job_;
+      }
+      (*job)(w);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) done_cv_.notify_all();
+    }
+    in_section() = false;
+  }
+  void loop()
+  {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      work();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex mu_, run_mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)> *job_ = nullptr;
+  int n_ = 0, next_ = 0, left_ = 0;
+  uint64_t gen_ = 0;
+};
+
 // Run fn(lo, hi) over [0, n) split into contiguous ranges on up to
-// host_threads() threads (the calling thread takes the first range).
+// host_threads() pool threads (the calling thread takes part).
 template <typename F>
 static void parallel_ranges(size_t n, F fn, size_t min_per_thread = 256)
 {
-  const size_t nthr = std::max<size_t>(1, std::min<size_t>((size_t)host_threads(), n / min_per_thread));
+  const size_t nthr = std::max<size_t>(
+      1, std::min<size_t>(std::min<size_t>((size_t)host_threads(), (size_t)HostPool::get().size()), n / min_per_thread));
   if (nthr <= 1) {
     fn((size_t)0, n);
     return;
   }
-  std::vector<std::thread> pool;
-  for (size_t w = 1; w < nthr; w++) pool.emplace_back(fn, n * w / nthr, n * (w + 1) / nthr);
-  fn((size_t)0, n / nthr);
-  for (auto &t : pool) t.join();
+  HostPool::get().run((int)nthr, [&](int w) { fn(n * w / nthr, n * (w + 1) / nthr); });
 }
 
 static BlockCache &block_cache()
@@ -155,19 +246,15 @@ static BlockCache &block_cache()
 // are bound by page faults and one core's copy rate).
 static void host_copy(void *dst, const void *src, size_t n)
 {
-  const size_t parts = std::min<size_t>(8, std::max<size_t>(1, n >> 21));   // 2 MB or more per thread
+  const size_t parts = std::min<size_t>((size_t)HostPool::get().size(), std::max<size_t>(1, n >> 20));   // 1 MB or more each
   if (parts <= 1) {
     memcpy(dst, src, n);
     return;
   }
-  std::vector<std::thread> pool;
-  for (size_t w = 1; w < parts; w++)
-    pool.emplace_back([=] {
-      const size_t a = n * w / parts, b = n * (w + 1) / parts;
-      memcpy((char *)dst + a, (const char *)src + a, b - a);
-    });
-  memcpy(dst, src, n / parts);
-  for (auto &t : pool) t.join();
+  HostPool::get().run((int)parts, [=](int w) {
+    const size_t a = n * w / parts, b = n * (w + 1) / parts;
+    memcpy((char *)dst + a, (const char *)src + a, b - a);
+  });
 }
 
 struct PinnedStage {
@@ -222,6 +309,45 @@ struct PinnedStage {
   }
 
 };
+
+// Pinned host arenas for the uploads of an engine's creation, kept for the
+// process and shared by creations one at a time each: a large upload is
+// copied into the creation's arena (on the host pool) and sent from there at
+// the link's speed, and the arena is handed back once the creation's set-up
+// stream has drained.  A pageable upload goes through the driver's own
+// staging, one core at a time (about 7 GB/s here).
+struct PinnedArenas {
+  static constexpr size_t kArena = 128u << 20;
+  std::mutex mu;
+  std::vector<char *> free_list;
+  char *take()
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!free_list.empty()) {
+      char *a = free_list.back();
+      free_list.pop_back();
+      return a;
+    }
+    char *a = nullptr;
+    if (cudaHostAlloc((void **)&a, kArena, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return a;
+  }
+  void give(char *a)
+  {
+    if (!a) return;
+    std::lock_guard<std::mutex> lk(mu);
+    free_list.push_back(a);
+  }
+};
+
+static PinnedArenas &pinned_arenas()
+{
+  static PinnedArenas *a = new PinnedArenas;   // never destroyed: outlives every engine
+  return *a;
+}
 
 static PinnedStage &pinned_stage()
 {
@@ -599,13 +725,40 @@ struct Engine : EngineBase {
     if (s) cudaStreamDestroy(s);
   }
 
+  // This creation's pinned arena (null outside creation or when none could
+  // be pinned) and the bytes of it already handed out.
+  char *arena = nullptr;
+  size_t arena_used = 0;
+  static constexpr size_t kArenaMin = 256u << 10;   // smaller uploads go from pageable memory
+
+  // A 256-byte-aligned slice of the arena for bytes about to be uploaded on
+  // ss, or null if the arena is absent or full.
+  char *arena_slice(size_t bytes)
+  {
+    if (!arena || bytes < kArenaMin || arena_used + bytes > PinnedArenas::kArena) return nullptr;
+    char *a = arena + arena_used;
+    arena_used += (bytes + 255) / 256 * 256;
+    return a;
+  }
+
+  // bytes from host h to device d on the set-up stream.
+  int put(void *d, const void *h, size_t bytes)
+  {
+    if (!bytes) return 0;
+    if (char *a = arena_slice(bytes)) {
+      host_copy(a, h, bytes);
+      h = a;
+    }
+    CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ss));
+    stats.h2d_bytes += bytes;
+    return 0;
+  }
+
   template <typename U>
   int upload(U **d, const U *h, size_t n)
   {
     if (mem.alloc(d, n)) return VGPU_ENOMEM;
-    if (n) CK(cudaMemcpyAsync(*d, h, sizeof(U) * n, cudaMemcpyHostToDevice, ss));
-    stats.h2d_bytes += sizeof(U) * n;
-    return 0;
+    return put(*d, h, sizeof(U) * n);
   }
 
   // Copies n values into a device array of n + pad elements (zero tail), so
@@ -615,9 +768,7 @@ struct Engine : EngineBase {
     std::vector<T> tmp(n + pad ? n + pad : 1, (T)0);
     for (size_t q = 0; q < n; q++) tmp[q] = (T)h[q];
     if (mem.alloc(d, n + pad)) return VGPU_ENOMEM;
-    if (n + pad) CK(cudaMemcpyAsync(*d, tmp.data(), sizeof(T) * (n + pad), cudaMemcpyHostToDevice, ss));
-    stats.h2d_bytes += sizeof(T) * (n + pad);
-    return 0;
+    return put(*d, tmp.data(), sizeof(T) * (n + pad));
   }
 
   // Host volume [n0][n1][n2] -> padded device volume.
@@ -630,9 +781,7 @@ struct Engine : EngineBase {
         T *dst = tmp.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
         for (int k = 0; k < p.n[2]; k++) dst[k] = (T)src[k];
       }
-    CK(cudaMemcpyAsync(d, tmp.data(), sizeof(T) * vol, cudaMemcpyHostToDevice, ss));
-    stats.h2d_bytes += sizeof(T) * vol;
-    return 0;
+    return put(d, tmp.data(), sizeof(T) * vol);
   }
 
   // With VGPU_TRACE set, create() prints the time of each set-up phase.
@@ -659,7 +808,13 @@ struct Engine : EngineBase {
   {
     PhaseClock pc;
     g_creating++;
+    arena = pinned_arenas().take();
+    arena_used = 0;
     int rc = create_phases(in, pc);
+    // Every copy out of the arena has finished before it is handed back.
+    if (ss) cudaStreamSynchronize(ss);
+    pinned_arenas().give(arena);
+    arena = nullptr;
     g_creating--;
     pclock = nullptr;
     pc.print(vol);
@@ -1115,12 +1270,7 @@ struct Engine : EngineBase {
           }
     };
     mark(efield ? "tfsf-e-start" : "tfsf-h-start");
-    {
-      std::vector<std::thread> pool;
-      for (int q = 1; q < tv.n; q++) pool.emplace_back(enumerate, q);
-      if (tv.n > 0) enumerate(0);
-      for (auto &t : pool) t.join();
-    }
+    HostPool::get().run(tv.n, enumerate);
     mark("enumerate");
     // Points of one entry first, then the multi-entry points' runs.
     size_t ns = 0, nm = 0;
@@ -1145,10 +1295,7 @@ struct Engine : EngineBase {
         std::copy(pt.multi.begin(), pt.multi.end(), ent.begin() + moff[q]);
         std::copy(pt.mpos.begin(), pt.mpos.end(), pos.begin() + 3 * moff[q]);
       };
-      std::vector<std::thread> pool;
-      for (int q = 1; q < tv.n; q++) pool.emplace_back(place, q);
-      if (tv.n > 0) place(0);
-      for (auto &t : pool) t.join();
+      HostPool::get().run(tv.n, place);
     }
     for (int q = 0; q < tv.n; q++)
       for (int m : parts[q].mstart) mstart.push_back((int)moff[q] + m);
@@ -1201,10 +1348,27 @@ struct Engine : EngineBase {
       uint64_t lastraw[6] = {};   // bit patterns of the previous cell's doubles
       const double *src[6];
       for (int c = 0; c < count; c++) src[c] = p.coef[first + c];
+      int64_t prev_hrow = -1;
+      const uint8_t *prev_irow = nullptr;
       for (int i = i0; i < i1 && !pt.overflow; i++)
         for (int j = 0; j < p.n[1]; j++) {
           const int64_t hrow = ((int64_t)i * p.n[1] + j) * p.n[2];
           uint8_t *irow = idx.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
+          // A row whose doubles equal the row before (the common case):
+          // the same tuples, compared and copied a row at a time.
+          if (prev_irow) {
+            bool same = true;
+            for (int c = 0; c < count && same; c++)
+              same = memcmp(src[c] + hrow, src[c] + prev_hrow, sizeof(double) * (size_t)p.n[2]) == 0;
+            if (same) {
+              memcpy(irow, prev_irow, (size_t)p.n[2]);
+              prev_hrow = hrow;
+              prev_irow = irow;
+              continue;
+            }
+          }
+          prev_hrow = hrow;
+          prev_irow = irow;
           for (int k = 0; k < p.n[2]; k++) {
             // Same doubles as the previous cell (the common case): same tuple.
             uint64_t raw[6];
@@ -1237,10 +1401,7 @@ struct Engine : EngineBase {
           }
         }
     };
-    std::vector<std::thread> pool;
-    for (int w = 1; w < nthr; w++) pool.emplace_back(work, w);
-    work(0);
-    for (auto &t : pool) t.join();
+    HostPool::get().run(nthr, work);
     // Merge: global numbers in plane order, then renumber each part's planes.
     std::map<Key, int> global;
     std::vector<T> table;
@@ -1341,63 +1502,30 @@ struct Engine : EngineBase {
 
 
   // Per-tile headers (see SweepHeader): membership masks, line lengths and
-  // UPML profiles, in the storage type, as the device arrays hold them.
+  // UPML profiles, built on the device (k_headers) from the uploaded tiles
+  // and the storage-type line and profile arrays the engine already holds.
   template <bool ES, bool PML>
-  int build_headers(SweepLaunch &L, const std::vector<SweepTile> &tiles)
+  int build_headers(SweepLaunch &L)
   {
     using Hdr = SweepHeader<T, PML>;
-    std::vector<Hdr> hv(tiles.size());
-    const Box *bb = ES ? be : bh;
-    const double *const *lines = ES ? p.idh : p.ide;
-    const double *const *prof[4] = { ES ? p.pml_ad : p.pml_ah, ES ? p.pml_bd : p.pml_bh, ES ? p.pml_ah : p.pml_ad,
-                                     ES ? p.pml_ibh : p.pml_ibd };
-    auto bits = [&](const SweepTile &t, int v, int axis) {
-      auto in = [&](const Box &b) {
-        const int lo = axis == 0 ? b.i0 : axis == 1 ? b.j0 : b.k0, hi = axis == 0 ? b.i1 : axis == 1 ? b.j1 : b.k1;
-        return (v >= lo && v <= hi) ? 1u : 0u;
-      };
-      uint32_t m = 0;
-      for (int c = 0; c < 3; c++) {
-        if (t.bulk) m |= in(bb[c]) << c;
-        if (PML && t.reg[0] >= 0) m |= in(pv.lim[t.reg[0]][(ES ? EX : HX) + c]) << (3 + c);
-        if (PML && t.reg[1] >= 0) m |= in(pv.lim[t.reg[1]][(ES ? EX : HX) + c]) << (6 + c);
-      }
-      return m;
-    };
-    auto at = [&](const double *a, int axis, int v) { return (a && v >= 0 && v < p.n[axis]) ? (T)a[v] : (T)0; };
-    // Tiles are independent: host threads take contiguous ranges.
-    parallel_ranges(tiles.size(), [&](size_t q0, size_t q1) {
-    for (size_t q = q0; q < q1; q++) {
-      const SweepTile &t = tiles[q];
-      Hdr &h = hv[q];
-      memset(&h, 0, sizeof h);
-      h.t = t;
-      const int n = t.i1 - t.i0 + 1;
-      for (int e = 0; e < kSweepMaxPlanes; e++) {
-        const int i = ES ? t.i0 + e : t.i1 - e;
-        h.plane_mask[e] = e < n ? bits(t, i, 0) : 0u;
-        h.dx[e] = at(lines[0], 0, i);
-        if (PML)
-          for (int a = 0; a < 4; a++) h.px[a][e] = at(prof[a][0], 0, i);
-      }
-      for (int r = 0; r < kSweepJH; r++) {
-        const int j = t.j0 + r;
-        h.row_mask[r] = j < p.n[1] ? bits(t, j, 1) : 0u;
-        h.dy[r] = at(lines[1], 1, j);
-        if (PML)
-          for (int a = 0; a < 4; a++) h.py[a][r] = at(prof[a][1], 1, j);
-      }
-      for (int c = 0; c < kSweepKW; c++) {
-        const int k = t.k0 + c;
-        h.col_mask[c] = bits(t, k, 2);
-        h.dz[c] = at(lines[2], 2, k);
-        if (PML)
-          for (int a = 0; a < 4; a++) h.pz[a][c] = at(prof[a][2], 2, k);
-      }
-    }
-    });
     Hdr *d = nullptr;
-    if (upload(&d, hv.data(), hv.size())) return VGPU_ENOMEM;
+    if (mem.alloc(&d, (size_t)L.ntiles)) return VGPU_ENOMEM;
+    HeaderBoxes hb{};
+    const Box *bb = ES ? be : bh;
+    for (int c = 0; c < 3; c++) hb.bulk[c] = bb[c];
+    for (int q = 0; q < pv.nreg; q++)
+      for (int c = 0; c < 3; c++) hb.reg[q][c] = pv.lim[q][(ES ? EX : HX) + c];
+    HeaderLines<T> hl{};
+    for (int a = 0; a < 3; a++) {
+      hl.line[a] = ES ? g.idh[a] : g.ide[a];
+      hl.prof[0][a] = ES ? pv.ad[a] : pv.ah[a];
+      hl.prof[1][a] = ES ? pv.bd[a] : pv.bh[a];
+      hl.prof[2][a] = ES ? pv.ah[a] : pv.ad[a];
+      hl.prof[3][a] = ES ? pv.ibh[a] : pv.ibd[a];
+      hl.n[a] = p.n[a];
+    }
+    k_headers<T, ES, PML><<<L.ntiles, 32, 0, ss>>>(L.tiles, L.ntiles, hb, hl, d);
+    CK(cudaGetLastError());
     L.headers = d;
     return 0;
   }
@@ -1412,7 +1540,7 @@ struct Engine : EngineBase {
         return set_err(VGPU_EINVAL, "sweep tile of %d planes at k0=%d", t.i1 - t.i0 + 1, t.k0);
     if (upload(&L.tiles, tiles.data(), tiles.size())) return VGPU_ENOMEM;
     L.host = tiles;
-    if (int rc = build_headers<ES, PML>(L, tiles)) return rc;
+    if (int rc = build_headers<ES, PML>(L)) return rc;
     L.smem = SweepLayout<T, ES, PML>::smem_bytes(compressed);
     auto kern = k_sweep_tma<T, ES, PML>;
     // The attribute is per kernel, shared by every engine in the process:

@@ -190,6 +190,67 @@ struct alignas(16) SweepHeader {
 
 __host__ __device__ constexpr uint32_t round128(uint32_t b) { return (b + 127u) / 128u * 128u; }
 
+// What k_headers needs beside the tiles: the sweep's components' bulk boxes
+// and UPML region boxes, the line lengths (E sweep: idh; H sweep: ide) and
+// the four UPML profiles (a, b, c, d) per axis, all in the storage type.
+struct HeaderBoxes {
+  Box bulk[3];
+  Box reg[6][3];   // [region][component]
+};
+
+template <typename T>
+struct HeaderLines {
+  const T *line[3];
+  const T *prof[4][3];
+  int n[3];
+};
+
+// The headers of a tile list (SweepHeader), one warp per tile: lane l fills
+// plane l of the march, row l (l < 8) and column l.  A value outside the
+// grid is 0; a plane past the tile's last has an empty mask.
+template <typename T, bool ES, bool PML>
+__global__ void k_headers(const SweepTile *__restrict__ tiles, int ntiles, HeaderBoxes hb, HeaderLines<T> hl,
+                          SweepHeader<T, PML> *__restrict__ out)
+{
+  const int q = blockIdx.x, l = threadIdx.x;
+  if (q >= ntiles) return;
+  const SweepTile t = tiles[q];
+  SweepHeader<T, PML> &h = out[q];
+  auto bits = [&](int v, int axis) {
+    auto in = [&](const Box &b) -> uint32_t {
+      const int lo = axis == 0 ? b.i0 : axis == 1 ? b.j0 : b.k0, hi = axis == 0 ? b.i1 : axis == 1 ? b.j1 : b.k1;
+      return (v >= lo && v <= hi) ? 1u : 0u;
+    };
+    uint32_t m = 0;
+    for (int c = 0; c < 3; c++) {
+      if (t.bulk) m |= in(hb.bulk[c]) << c;
+      if (PML && t.reg[0] >= 0) m |= in(hb.reg[t.reg[0]][c]) << (3 + c);
+      if (PML && t.reg[1] >= 0) m |= in(hb.reg[t.reg[1]][c]) << (6 + c);
+    }
+    return m;
+  };
+  auto at = [&](const T *a, int axis, int v) { return (a && v >= 0 && v < hl.n[axis]) ? a[v] : (T)0; };
+  if (l == 0) h.t = t;
+  const int n = t.i1 - t.i0 + 1;
+  const int i = ES ? t.i0 + l : t.i1 - l;
+  h.plane_mask[l] = l < n ? bits(i, 0) : 0u;
+  h.dx[l] = at(hl.line[0], 0, i);
+  if (PML)
+    for (int a = 0; a < 4; a++) h.px[a][l] = at(hl.prof[a][0], 0, i);
+  if (l < kSweepJH) {
+    const int j = t.j0 + l;
+    h.row_mask[l] = j < hl.n[1] ? bits(j, 1) : 0u;
+    h.dy[l] = at(hl.line[1], 1, j);
+    if (PML)
+      for (int a = 0; a < 4; a++) h.py[a][l] = at(hl.prof[a][1], 1, j);
+  }
+  const int k = t.k0 + l;
+  h.col_mask[l] = bits(k, 2);
+  h.dz[l] = at(hl.line[2], 2, k);
+  if (PML)
+    for (int a = 0; a < 4; a++) h.pz[a][l] = at(hl.prof[a][2], 2, k);
+}
+
 // ---- grouped sweeps: one launch over the tiles of many meshes ------------
 //
 // A group launch takes a list of tiles drawn from many independent meshes of
