@@ -452,13 +452,20 @@ def run_gpu_arm(args):
         return dict(td=td_, re=re_, im=im_, create_s=t1 - t0, step_s=t2 - t1, read_s=t3 - t2, wall_s=t3 - t0,
                     h2d=int(s_.h2d_bytes), d2h=td_.nbytes + re_.nbytes + im_.nbytes, run_ms=s_.run_ms)
 
+    # One untimed pass first (allocator caches, page-locked result blocks),
+    # as the W warm-up steps precede the timed ones.
+    e2e_run(prec, args.steps)
     k = e2e_run(prec, args.steps)
     e2e_wall = max_over_ranks(k["wall_s"], dist)
     e2e = {"value": world * n_out * args.steps / e2e_wall / 1e6, "unit": "Mcell-updates/s",
            "h2d_bytes_per_step": k["h2d"] / args.steps, "d2h_bytes_per_step": k["d2h"] / args.steps,
            "wall_s": e2e_wall, "create_s": k["create_s"], "step_s": k["step_s"], "read_s": k["read_s"],
            "what": f"vgpu_create (problem upload, {k['h2d']} bytes host->device) + K steps + observer read-back; "
-                   f"at K = {args.steps} creation is {100 * k['create_s'] / k['wall_s']:.0f}% of the wall time"}
+                   f"at K = {args.steps} creation is {100 * k['create_s'] / k['wall_s']:.0f}% of the wall time; "
+                   "one untimed pass before it"}
+    # Its results go: their page-locked blocks return to the cache for the
+    # next read.
+    k = None
 
     # The workload's whole run (its own 4000 steps) end to end, and the same
     # run in plain FP64: the FP32 error per result against it, and the FP64

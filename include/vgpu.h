@@ -350,6 +350,16 @@ int vgpu_run_grouped(vgpu_engine *const *engines, int32_t n, const uint64_t *ste
  * most 64 distinct tuples; 0 if not; a negative status on error. */
 int vgpu_groupable(const vgpu_engine *engine);
 
+/* Page-locked host memory for read-backs, from blocks the library caches
+ * for the process (pinning costs milliseconds per megabyte).  A DFT read
+ * (vgpu_read_dft) into such memory goes straight from the device at the
+ * link's speed; one into pageable memory is staged and copied on the host,
+ * where the copy into freshly allocated pages costs more than the transfer.
+ * vgpu_host_alloc returns NULL when no block can be had; vgpu_host_free
+ * returns a block to the cache (at most 2 GB are kept). */
+void *vgpu_host_alloc(uint64_t bytes);
+void vgpu_host_free(void *ptr);
+
 /* Sweep tuning for the engines the calling thread creates afterwards and
  * the groups it runs: march_depth planes per tile (1..32; 0 restores the
  * built-in rule of about 16 tiles per SM), at most blocks_per_sm resident

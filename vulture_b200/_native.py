@@ -102,6 +102,8 @@ def lib() -> C.CDLL:
                                        C.POINTER(VgpuGroupReport)]),
         "vgpu_groupable": (C.c_int, [P]),
         "vgpu_set_sweep_tuning": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
+        "vgpu_host_alloc": (C.c_void_p, [C.c_uint64]),
+        "vgpu_host_free": (None, [C.c_void_p]),
         "vgpu_destroy": (None, [P]),
         "vgpu_last_error": (C.c_char_p, []),
     }
@@ -133,7 +135,7 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
            "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device",
            "vgpu_check_sweep_plan", "vgpu_set_sweep_wait_limit", "vgpu_run_grouped", "vgpu_groupable",
-           "vgpu_set_sweep_tuning"]
+           "vgpu_set_sweep_tuning", "vgpu_host_alloc", "vgpu_host_free"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3
 # Other parts of a step and the 64-step DFT fold, for vgpu_time_kernel.

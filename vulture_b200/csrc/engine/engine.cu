@@ -349,6 +349,67 @@ static PinnedArenas &pinned_arenas()
   return *a;
 }
 
+// Page-locked host blocks for read-backs (vgpu_host_alloc), cached for the
+// process: pinning costs milliseconds per megabyte, so a freed block is kept
+// for the next request of about its size, up to 2 GB in all.
+struct HostBlocks {
+  static constexpr size_t kCacheMax = (size_t)2 << 30;
+  std::mutex mu;
+  std::multimap<size_t, void *> free_blocks;
+  std::map<void *, size_t> sizes;   // every block handed out or cached
+  size_t cached = 0;
+  void *alloc(size_t b)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = free_blocks.lower_bound(b);
+    if (it != free_blocks.end() && it->first <= 2 * b + ((size_t)1 << 20)) {
+      void *q = it->second;
+      cached -= it->first;
+      free_blocks.erase(it);
+      return q;
+    }
+    void *q = nullptr;
+    if (cudaHostAlloc(&q, b ? b : 1, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    sizes[q] = b;
+    return q;
+  }
+  void release(void *q)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto s = sizes.find(q);
+    if (s == sizes.end()) return;
+    free_blocks.emplace(s->second, q);
+    cached += s->second;
+    while (cached > kCacheMax && !free_blocks.empty()) {
+      auto big = std::prev(free_blocks.end());
+      cudaFreeHost(big->second);
+      cached -= big->first;
+      sizes.erase(big->second);
+      free_blocks.erase(big);
+    }
+  }
+};
+
+static HostBlocks &host_blocks()
+{
+  static HostBlocks *h = new HostBlocks;   // never destroyed: outlives every engine
+  return *h;
+}
+
+// Whether host memory is page-locked (a read into it needs no staging).
+static bool is_pinned(const void *ptr)
+{
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 static PinnedStage &pinned_stage()
 {
   static PinnedStage *st = new PinnedStage;   // never destroyed: outlives every engine
@@ -2280,8 +2341,15 @@ struct Engine : EngineBase {
     if (!n) return 0;
     if (int rc = fold_pending()) return rc;
     CK(cudaStreamSynchronize(s));
-    if (int rc = pinned_stage().d2h(re, d_re, sizeof(double) * n, s)) return rc;
-    if (int rc = pinned_stage().d2h(im, d_im, sizeof(double) * n, s)) return rc;
+    // Into page-locked memory the sums go straight from the device.
+    if (is_pinned(re) && is_pinned(im)) {
+      CK(cudaMemcpyAsync(re, d_re, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(im, d_im, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    } else {
+      if (int rc = pinned_stage().d2h(re, d_re, sizeof(double) * n, s)) return rc;
+      if (int rc = pinned_stage().d2h(im, d_im, sizeof(double) * n, s)) return rc;
+    }
     return 0;
   }
 
@@ -3114,6 +3182,13 @@ extern "C" int vgpu_run_batch(vgpu_engine *const *engines, int32_t n, const uint
   }
   if (rc) set_err(rc, "%s", msg.c_str());
   return rc;
+}
+
+extern "C" void *vgpu_host_alloc(uint64_t bytes) { return host_blocks().alloc((size_t)bytes); }
+
+extern "C" void vgpu_host_free(void *ptr)
+{
+  if (ptr) host_blocks().release(ptr);
 }
 
 extern "C" int vgpu_set_sweep_tuning(int32_t march_depth, int32_t blocks_per_sm, int32_t group_chunk)

@@ -133,6 +133,36 @@ class Mesh:
         self.bin_end()
 
 
+class _HostBlock:
+    """Owner of a page-locked host block from the library's cache, exposed to
+    numpy: the array keeps this object alive and the block returns to the
+    cache when the array goes."""
+
+    def __init__(self, shape, dtype):
+        nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = N.lib().vgpu_host_alloc(nbytes)
+        self.__array_interface__ = {"shape": tuple(shape), "typestr": np.dtype(dtype).str,
+                                    "data": (self.ptr or 0, False), "version": 3}
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                N.lib().vgpu_host_free(self.ptr)
+        except Exception:
+            pass
+
+
+def _result_array(shape, dtype=np.float64):
+    """An uninitialised array for a large read-back: page-locked, so the
+    device writes it directly (a fresh pageable array costs a page fault per
+    4 KB as the staged copy first touches it); small ones are plain numpy."""
+    if int(np.prod(shape)) * np.dtype(dtype).itemsize >= (4 << 20):
+        blk = _HostBlock(shape, dtype)
+        if blk.ptr:
+            return np.asarray(blk)
+    return np.empty(shape, dtype)
+
+
 class GpuRun:
     """An engine instance on the current CUDA device (vgpu_create/run)."""
 
@@ -227,8 +257,8 @@ class GpuRun:
             z = np.zeros((max(m.num_fd, 1), 6, max(m.num_freq, 1)))
             return z, z.copy()
         # Filled entirely by the read: no zero-fill of a buffer about to be overwritten.
-        re = np.empty((m.num_fd, 6, max(m.num_freq, 1)))
-        im = np.empty_like(re)
+        re = _result_array((m.num_fd, 6, max(m.num_freq, 1)))
+        im = _result_array(re.shape)
         N.check_gpu(N.lib().vgpu_read_dft(self._e, re.ctypes.data, im.ctypes.data))
         return re, im
 
