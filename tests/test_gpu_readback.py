@@ -36,7 +36,7 @@ def test_dft_read_pinned_equals_pageable():
 
 def test_host_blocks_are_cached():
     L = N.lib()
-    n = 6 << 20
+    n = (13 << 20) + 4096   # a size no other test asks for: the cache holds none like it
     a = L.vgpu_host_alloc(n)
     assert a
     C.memset(a, 7, n)
@@ -45,6 +45,6 @@ def test_host_blocks_are_cached():
     assert b == a
     L.vgpu_host_free(b)
     arr = _result_array((n // 8,))
-    assert arr.nbytes == n
+    assert arr.nbytes == n and arr.ctypes.data == a
     arr[:] = 1.5
     assert float(arr.sum()) == 1.5 * (n // 8)

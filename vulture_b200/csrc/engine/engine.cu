@@ -806,10 +806,12 @@ struct Engine : EngineBase {
   int put(void *d, const void *h, size_t bytes)
   {
     if (!bytes) return 0;
-    if (char *a = arena_slice(bytes)) {
-      host_copy(a, h, bytes);
-      h = a;
-    }
+    const bool in_arena = arena && (const char *)h >= arena && (const char *)h < arena + PinnedArenas::kArena;
+    if (!in_arena)
+      if (char *a = arena_slice(bytes)) {
+        host_copy(a, h, bytes);
+        h = a;
+      }
     CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ss));
     stats.h2d_bytes += bytes;
     return 0;
@@ -1346,15 +1348,27 @@ struct Engine : EngineBase {
       soff[q + 1] = soff[q] + parts[q].single.size();
       moff[q + 1] = moff[q] + parts[q].multi.size();
     }
-    std::vector<TfsfEntry<T>> ent(ne);
-    std::vector<int> pos(3 * ne), mstart;
+    // The merged lists are written where they are sent from: the
+    // creation's pinned arena when it has room.
+    std::vector<TfsfEntry<T>> ent_v;
+    std::vector<int> pos_v, mstart;
+    TfsfEntry<T> *ent = (TfsfEntry<T> *)arena_slice(sizeof(TfsfEntry<T>) * ne);
+    int *pos = (int *)arena_slice(sizeof(int) * 3 * ne);
+    if (!ent) {
+      ent_v.resize(ne);
+      ent = ent_v.data();
+    }
+    if (!pos) {
+      pos_v.resize(3 * ne);
+      pos = pos_v.data();
+    }
     {
       auto place = [&](int q) {
         const Part &pt = parts[q];
-        std::copy(pt.single.begin(), pt.single.end(), ent.begin() + soff[q]);
-        std::copy(pt.spos.begin(), pt.spos.end(), pos.begin() + 3 * soff[q]);
-        std::copy(pt.multi.begin(), pt.multi.end(), ent.begin() + moff[q]);
-        std::copy(pt.mpos.begin(), pt.mpos.end(), pos.begin() + 3 * moff[q]);
+        std::copy(pt.single.begin(), pt.single.end(), ent + soff[q]);
+        std::copy(pt.spos.begin(), pt.spos.end(), pos + 3 * soff[q]);
+        std::copy(pt.multi.begin(), pt.multi.end(), ent + moff[q]);
+        std::copy(pt.mpos.begin(), pt.mpos.end(), pos + 3 * moff[q]);
       };
       HostPool::get().run(tv.n, place);
     }
@@ -1368,7 +1382,7 @@ struct Engine : EngineBase {
     if (!ne) return 0;
     TfsfEntry<T> *de;
     int *dpos, *dm;
-    if (upload(&de, ent.data(), ne) || upload(&dpos, pos.data(), 3 * ne) || upload(&dm, mstart.data(), mstart.size()))
+    if (upload(&de, ent, ne) || upload(&dpos, pos, 3 * ne) || upload(&dm, mstart.data(), mstart.size()))
       return VGPU_ENOMEM;
     tl.ent = de;
     tl.pos = dpos;
@@ -1376,7 +1390,6 @@ struct Engine : EngineBase {
     mark("upload");
     k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, ss>>>(g, L.pv, tv, tl, efield ? 1 : 0);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(ss));
     mark("prepare");
     return 0;
   }
@@ -1395,7 +1408,14 @@ struct Engine : EngineBase {
     };
     const int n0 = p.n[0];
     const int nthr = std::max(1, std::min<int>(host_threads(), n0));
-    std::vector<uint8_t> idx((size_t)vol, 0);
+    // Written where it is sent from: the creation's pinned arena when it has
+    // room (the row padding past n2 is never read).
+    std::vector<uint8_t> idx_v;
+    uint8_t *idx = (uint8_t *)arena_slice((size_t)vol);
+    if (!idx) {
+      idx_v.assign((size_t)vol, 0);
+      idx = idx_v.data();
+    }
     struct Part {
       std::vector<Key> keys;   // local tuples in first-seen order
       bool overflow = false;
@@ -1414,7 +1434,7 @@ struct Engine : EngineBase {
       for (int i = i0; i < i1 && !pt.overflow; i++)
         for (int j = 0; j < p.n[1]; j++) {
           const int64_t hrow = ((int64_t)i * p.n[1] + j) * p.n[2];
-          uint8_t *irow = idx.data() + (int64_t)i * g.s0 + (int64_t)j * g.s1;
+          uint8_t *irow = idx + (int64_t)i * g.s0 + (int64_t)j * g.s1;
           // A row whose doubles equal the row before (the common case):
           // the same tuples, compared and copied a row at a time.
           if (prev_irow) {
@@ -1468,7 +1488,7 @@ struct Engine : EngineBase {
     std::vector<T> table;
     for (int w = 0; w < nthr; w++) {
       if (parts[w].overflow) return 0;  // too many: keep the full volumes
-      uint8_t remap[256];
+      uint8_t remap[256] = {};
       for (size_t q = 0; q < parts[w].keys.size(); q++) {
         const Key &key = parts[w].keys[q];
         auto it = global.find(key);
@@ -1487,7 +1507,7 @@ struct Engine : EngineBase {
     }
     uint8_t *d_idx;
     T *d_tab;
-    if (upload(&d_idx, idx.data(), idx.size()) || upload(&d_tab, table.data(), table.size())) return VGPU_ENOMEM;
+    if (upload(&d_idx, idx, (size_t)vol) || upload(&d_tab, table.data(), table.size())) return VGPU_ENOMEM;
     out.idx = d_idx;
     out.table = d_tab;
     out.ntab = (int)global.size();
