@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define VGPU_ABI_VERSION 2
+#define VGPU_ABI_VERSION 3
 
 /* Status codes. */
 #define VGPU_OK            0
@@ -229,6 +229,19 @@ typedef struct {
    * vgpu_bin_sink. */
   int64_t num_bin;
   const int32_t *bin_points;  /* [num_bin][3] grid indices */
+
+  /* Optional medium tags, the reference's USE_INDEXED_MEDIA idea
+   * (src/grid.h:108-136) kept beside the volumes.  coef_tag[f] holds one byte
+   * per cell for component f (Ex, Ey, Ez, Hx, Hy, Hz): 0 where the
+   * component's coefficients are zero, t > 0 where they are tag_coef[t - 1]'s
+   * -- alpha and beta (coef[f], coef[3 + f]) for an E component, gamma
+   * (coef[3 + f]) for an H one.  When set they must describe coef[] exactly;
+   * vgpu_create then finds the distinct coefficient tuples from three bytes
+   * per cell for E and three for H instead of the nine double volumes.  All
+   * NULL (or num_tags 0): it scans coef[]. */
+  const uint8_t *coef_tag[6];
+  int32_t num_tags;           /* at most 255 */
+  const double *tag_coef;     /* [num_tags][3]: alpha, beta, gamma */
 } vgpu_problem;
 
 typedef struct vgpu_engine vgpu_engine;

@@ -44,6 +44,20 @@ double vhost_dt(const vhost *h);
 /* Outer-box cell count, the reference's spi/cell denominator (src/timer.c:95). */
 uint64_t vhost_num_cells(const vhost *h);
 
+/* No counterpart in the reference.  The set-up paints a one-byte medium tag
+ * per cell and component beside the coefficient volumes and hands both to
+ * the engine (vgpu_problem.coef_tag).  use = 0 leaves the tags out of the
+ * problem, so that the engine finds the coefficient tuples by scanning the
+ * volumes; use = 1 puts them back.  The engine's results are the same either
+ * way. */
+int vhost_use_tags(vhost *h, int32_t use);
+
+/* No counterpart in the reference.  The number of (cell, component) pairs
+ * whose tag does not give the coefficient volumes' values bit for bit; -1
+ * when the set-up keeps no tags (more than 255 distinct coefficient
+ * triples). */
+int64_t vhost_check_tags(const vhost *h);
+
 /* Write eh_<name>_td.asc / eh_<name>_fd.asc / wf_<name>_td.asc /
  * wf_<name>_fd.asc into the current directory from the engine's samples
  * (td: [steps][num_td][6]) and DFTs (re/im: [num_fd][6][num_freq]).

@@ -67,6 +67,8 @@ def lib() -> C.CDLL:
         "vhost_num_freq": (C.c_int32, [P]),
         "vhost_dt": (C.c_double, [P]),
         "vhost_num_cells": (C.c_uint64, [P]),
+        "vhost_use_tags": (C.c_int, [P, C.c_int32]),
+        "vhost_check_tags": (C.c_int64, [P]),
         "vhost_write_outputs": (C.c_int, [P, P, C.c_uint64, P, P, C.c_int32]),
         "vhost_observer_name": (C.c_char_p, [P, C.c_int32, C.c_int32]),
         "vhost_num_bin": (C.c_int64, [P]),
@@ -135,7 +137,7 @@ EXPORTS = ["vhost_load", "vhost_problem", "vhost_num_steps", "vhost_num_output_s
            "vhost_bin_end", "vhost_write_lines", "vgpu_sweep_points", "vgpu_enqueue", "vgpu_query",
            "vgpu_synchronize", "vgpu_run_batch", "vgpu_set_device", "vgpu_get_device",
            "vgpu_check_sweep_plan", "vgpu_set_sweep_wait_limit", "vgpu_run_grouped", "vgpu_groupable",
-           "vgpu_set_sweep_tuning", "vgpu_host_alloc", "vgpu_host_free"]
+           "vgpu_set_sweep_tuning", "vgpu_host_alloc", "vgpu_host_free", "vhost_use_tags", "vhost_check_tags"]
 
 VGPU_K_BULK_E, VGPU_K_BULK_H, VGPU_K_PML_E, VGPU_K_PML_H = 0, 1, 2, 3
 # Other parts of a step and the 64-step DFT fold, for vgpu_time_kernel.

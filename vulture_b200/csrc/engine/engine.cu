@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -937,7 +938,7 @@ struct Engine : EngineBase {
     }
     if (mem.alloc(&d_step, 1)) return VGPU_ENOMEM;
     CK(cudaMemsetAsync(d_step, 0, sizeof(uint64_t), ss));
-    pc.mark("coef");
+    pc.mark(p.num_tags > 0 && p.tag_coef ? "coef-from-tags" : "coef");
 
     // Bulk limits.
     for (int c = 0; c < 3; c++) {
@@ -1284,12 +1285,28 @@ struct Engine : EngineBase {
     TfsfList<T> &tl = efield ? L.le : L.lh;
     // A point belongs to the first item (in face order) that holds it; the
     // later items of the same component that hold it follow it in its run.
-    // Items are enumerated on separate host threads and joined in item order.
+    // Each item's points, in its i, j, k order, are cut into ranges that are
+    // enumerated on separate host threads and joined in item and range order.
     struct Part {
+      int q;                                 // item
+      int64_t lo, hi;                        // range of the item's points
       std::vector<TfsfEntry<T>> single, multi;
       std::vector<int> spos, mpos, mstart;   // mstart: run starts within multi
     };
-    std::vector<Part> parts(tv.n);
+    std::vector<Part> parts;
+    {
+      int64_t total = 0;
+      for (int q = 0; q < tv.n; q++) total += tv.it[q].b.count();
+      const int64_t chunk = std::max<int64_t>(4096, total / (2 * host_threads()) + 1);
+      for (int q = 0; q < tv.n; q++)
+        for (int64_t lo = 0, n = tv.it[q].b.count(); lo < n; lo += chunk) {
+          parts.emplace_back();
+          parts.back().q = q;
+          parts.back().lo = lo;
+          parts.back().hi = std::min(n, lo + chunk);
+        }
+    }
+    const int nparts = (int)parts.size();
     auto make = [&](int q, int i, int j, int k, std::vector<TfsfEntry<T>> &ent, std::vector<int> &pos) {
       const TfsfItem &it = tv.it[q];
       // Line length and coefficients are filled in on the device
@@ -1303,37 +1320,46 @@ struct Engine : EngineBase {
       sp[it.axis] += it.shift;
       pos.insert(pos.end(), sp, sp + 3);
     };
-    auto enumerate = [&](int q) {
+    auto enumerate = [&](int w) {
+      Part &pt = parts[w];
+      const int q = pt.q;
       const TfsfItem &it = tv.it[q];
-      Part &pt = parts[q];
       // Other items of the component that meet this one.
       int others[12], no = 0;
       for (int e = 0; e < tv.n; e++)
         if (e != q && tv.it[e].c == it.c && boxes_meet(tv.it[e].b, it.b)) others[no++] = e;
-      pt.single.reserve(it.b.count());
-      pt.spos.reserve(3 * it.b.count());
-      for (int i = it.b.i0; i <= it.b.i1; i++)
-        for (int j = it.b.j0; j <= it.b.j1; j++)
-          for (int k = it.b.k0; k <= it.b.k1; k++) {
-            bool owned = true, followers = false;
-            for (int o = 0; o < no && owned; o++) {
-              if (!tv.it[others[o]].b.contains(i, j, k)) continue;
-              if (others[o] < q) owned = false;
-              else followers = true;
-            }
-            if (!owned) continue;
-            if (!followers) {
-              make(q, i, j, k, pt.single, pt.spos);
-              continue;
-            }
-            pt.mstart.push_back((int)pt.multi.size());
-            make(q, i, j, k, pt.multi, pt.mpos);
-            for (int o = 0; o < no; o++)
-              if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.multi, pt.mpos);
+      pt.single.reserve(pt.hi - pt.lo);
+      pt.spos.reserve(3 * (pt.hi - pt.lo));
+      const int64_t njk = (int64_t)it.b.nj() * it.b.nk();
+      int i = it.b.i0 + (int)(pt.lo / njk), j = it.b.j0 + (int)(pt.lo % njk / it.b.nk()),
+          k = it.b.k0 + (int)(pt.lo % it.b.nk());
+      for (int64_t x = pt.lo; x < pt.hi; x++) {
+        if (x > pt.lo && ++k > it.b.k1) {
+          k = it.b.k0;
+          if (++j > it.b.j1) {
+            j = it.b.j0;
+            i++;
           }
+        }
+        bool owned = true, followers = false;
+        for (int o = 0; o < no && owned; o++) {
+          if (!tv.it[others[o]].b.contains(i, j, k)) continue;
+          if (others[o] < q) owned = false;
+          else followers = true;
+        }
+        if (!owned) continue;
+        if (!followers) {
+          make(q, i, j, k, pt.single, pt.spos);
+          continue;
+        }
+        pt.mstart.push_back((int)pt.multi.size());
+        make(q, i, j, k, pt.multi, pt.mpos);
+        for (int o = 0; o < no; o++)
+          if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.multi, pt.mpos);
+      }
     };
     mark(efield ? "tfsf-e-start" : "tfsf-h-start");
-    HostPool::get().run(tv.n, enumerate);
+    HostPool::get().run(nparts, enumerate);
     mark("enumerate");
     // Points of one entry first, then the multi-entry points' runs.
     size_t ns = 0, nm = 0;
@@ -1343,8 +1369,8 @@ struct Engine : EngineBase {
     }
     const size_t ne = ns + nm;
     // Each part's runs go to their final offsets, one host thread per part.
-    std::vector<size_t> soff(tv.n + 1, 0), moff(tv.n + 1, ns);
-    for (int q = 0; q < tv.n; q++) {
+    std::vector<size_t> soff(nparts + 1, 0), moff(nparts + 1, ns);
+    for (int q = 0; q < nparts; q++) {
       soff[q + 1] = soff[q] + parts[q].single.size();
       moff[q + 1] = moff[q] + parts[q].multi.size();
     }
@@ -1370,9 +1396,9 @@ struct Engine : EngineBase {
         std::copy(pt.multi.begin(), pt.multi.end(), ent + moff[q]);
         std::copy(pt.mpos.begin(), pt.mpos.end(), pos + 3 * moff[q]);
       };
-      HostPool::get().run(tv.n, place);
+      HostPool::get().run(nparts, place);
     }
-    for (int q = 0; q < tv.n; q++)
+    for (int q = 0; q < nparts; q++)
       for (int m : parts[q].mstart) mstart.push_back((int)moff[q] + m);
     mstart.push_back((int)ne);
     mark("merge");
@@ -1421,6 +1447,74 @@ struct Engine : EngineBase {
       bool overflow = false;
     };
     std::vector<Part> parts(nthr);
+    // With medium tags a cell's tuple follows from its components' tag bytes
+    // (three per cell for E or H) instead of its doubles.  The cells are
+    // walked in the same order and each tuple is keyed by its values, so the
+    // index and the table are the ones the scan of the volumes gives.
+    // Volume q of coef[] is the alpha (q < 3), beta (q < 6) or gamma of the
+    // component whose tags are coef_tag[q < 3 ? q : q - 3].
+    bool tagged = p.num_tags > 0 && p.num_tags <= 255 && p.tag_coef;
+    for (int c = 0; c < count && tagged; c++) tagged = p.coef_tag[first + c < 3 ? first + c : first + c - 3] != nullptr;
+    auto work_tags = [&](int w) {
+      const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
+      Part &pt = parts[w];
+      std::map<Key, int> seen;
+      const int tv0 = first < 3 ? 0 : 3;     // the three tag volumes: tv0 .. tv0 + 2
+      const uint8_t *tg[3];
+      for (int c = 0; c < 3; c++) tg[c] = p.coef_tag[tv0 + c];
+      int vol_tag[6], vol_slot[6];
+      for (int c = 0; c < count; c++) {
+        const int q = first + c;
+        vol_tag[c] = (q < 3 ? q : q - 3) - tv0;
+        vol_slot[c] = q < 3 ? 0 : q < 6 ? 1 : 2;
+      }
+      int last = -1;
+      uint8_t lastt[3] = {};
+      int64_t prev_hrow = -1;
+      const uint8_t *prev_irow = nullptr;
+      for (int i = i0; i < i1 && !pt.overflow; i++)
+        for (int j = 0; j < p.n[1]; j++) {
+          const int64_t hrow = ((int64_t)i * p.n[1] + j) * p.n[2];
+          uint8_t *irow = idx + (int64_t)i * g.s0 + (int64_t)j * g.s1;
+          if (prev_irow && memcmp(tg[0] + hrow, tg[0] + prev_hrow, (size_t)p.n[2]) == 0 &&
+              memcmp(tg[1] + hrow, tg[1] + prev_hrow, (size_t)p.n[2]) == 0 &&
+              memcmp(tg[2] + hrow, tg[2] + prev_hrow, (size_t)p.n[2]) == 0) {
+            memcpy(irow, prev_irow, (size_t)p.n[2]);
+            prev_hrow = hrow;
+            prev_irow = irow;
+            continue;
+          }
+          prev_hrow = hrow;
+          prev_irow = irow;
+          for (int k = 0; k < p.n[2]; k++) {
+            const uint8_t t[3] = { tg[0][hrow + k], tg[1][hrow + k], tg[2][hrow + k] };
+            if (last >= 0 && t[0] == lastt[0] && t[1] == lastt[1] && t[2] == lastt[2]) {
+              irow[k] = (uint8_t)last;
+              continue;
+            }
+            Key key{};
+            for (int c = 0; c < count; c++) {
+              const uint8_t tc = t[vol_tag[c]];
+              key.v[c] = tc ? (T)p.tag_coef[(tc - 1) * 3 + vol_slot[c]] : (T)0.0;
+            }
+            int q = -1;
+            auto it = seen.find(key);
+            if (it != seen.end()) q = it->second;
+            if (q < 0) {
+              if (seen.size() == 256) {
+                pt.overflow = true;
+                return;
+              }
+              q = (int)seen.size();
+              seen.emplace(key, q);
+              pt.keys.push_back(key);
+            }
+            last = q;
+            memcpy(lastt, t, sizeof t);
+            irow[k] = (uint8_t)q;
+          }
+        }
+    };
     auto work = [&](int w) {
       const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
       Part &pt = parts[w];
@@ -1482,13 +1576,18 @@ struct Engine : EngineBase {
           }
         }
     };
-    HostPool::get().run(nthr, work);
+    if (tagged)
+      HostPool::get().run(nthr, work_tags);
+    else
+      HostPool::get().run(nthr, work);
     // Merge: global numbers in plane order, then renumber each part's planes.
     std::map<Key, int> global;
     std::vector<T> table;
+    std::vector<std::array<uint8_t, 256>> remap(nthr);
+    std::vector<char> ident(nthr, 1);
     for (int w = 0; w < nthr; w++) {
       if (parts[w].overflow) return 0;  // too many: keep the full volumes
-      uint8_t remap[256] = {};
+      remap[w].fill(0);
       for (size_t q = 0; q < parts[w].keys.size(); q++) {
         const Key &key = parts[w].keys[q];
         auto it = global.find(key);
@@ -1497,14 +1596,17 @@ struct Engine : EngineBase {
           it = global.emplace(key, (int)global.size()).first;
           for (int c = 0; c < count; c++) table.push_back(key.v[c]);
         }
-        remap[q] = (uint8_t)it->second;
+        remap[w][q] = (uint8_t)it->second;
+        ident[w] = ident[w] && it->second == (int)q;
       }
-      bool ident = true;
-      for (size_t q = 0; q < parts[w].keys.size(); q++) ident = ident && remap[q] == q;
-      if (ident) continue;
-      const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
-      for (int64_t x = (int64_t)i0 * g.s0; x < (int64_t)i1 * g.s0; x++) idx[x] = remap[idx[x]];
     }
+    // Each part renumbers its own planes, on its own thread.
+    HostPool::get().run(nthr, [&](int w) {
+      if (ident[w]) return;
+      const int i0 = (int)((int64_t)n0 * w / nthr), i1 = (int)((int64_t)n0 * (w + 1) / nthr);
+      const uint8_t *rm = remap[w].data();
+      for (int64_t x = (int64_t)i0 * g.s0; x < (int64_t)i1 * g.s0; x++) idx[x] = rm[idx[x]];
+    });
     uint8_t *d_idx;
     T *d_tab;
     if (upload(&d_idx, idx, (size_t)vol) || upload(&d_tab, table.data(), table.size())) return VGPU_ENOMEM;

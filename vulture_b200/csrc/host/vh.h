@@ -195,6 +195,13 @@ struct vhost {
   int grid_type;
   double dt;
   double *coef[9];
+  /* Medium tags of the six components (vgpu_problem.coef_tag): the painted
+   * (alpha, beta, gamma) triples in first-painted order; NULL once more than
+   * 255 distinct triples were painted. */
+  uint8_t *ctag[6];
+  int num_ctags;
+  double ctag_coef[255][3];
+  int tags_off;               /* vhost_use_tags(h, 0) */
   double pi, c0, mu0, eps0, eta0;
 
   /* PML (src/pml.c). */
@@ -257,6 +264,7 @@ void vh_log(vh_ctx *c, int verbose_only, const char *fmt, ...);
  * their release. */
 size_t vh_volume_bytes(size_t n);
 void vh_free_volume(double *p, size_t n);
+void vh_free_tags(vh_ctx *c);
 
 /* Runs fn(ctx, lo, hi) over [begin, end) split into contiguous ranges on
  * up to 16 threads; one call on the calling thread when work (the points

@@ -57,6 +57,7 @@ void vh_parallel_for(int begin, int end, int64_t work, void (*fn)(void *ctx, int
 }
 
 static double *alloc_volume(size_t n);
+static uint8_t *alloc_bytes(size_t n);
 
 int vh_outer_type(const vh_ctx *c, int face) { return c->bnds[c->ext_bnd[face]].type; }
 
@@ -201,6 +202,10 @@ int vh_init_grid(vh_ctx *c)
     c->coef[q] = alloc_volume((size_t)vol);
     if (!c->coef[q]) return vh_fail(c, "Failed to allocate grid coefficient arrays (%lld cells)", (long long)vol);
   }
+  /* Tags are an aid, not state: without memory for them the engine scans
+   * the volumes instead. */
+  for (int f = 0; f < 6; f++) c->ctag[f] = alloc_bytes((size_t)vol);
+  if (!c->ctag[0] || !c->ctag[1] || !c->ctag[2] || !c->ctag[3] || !c->ctag[4] || !c->ctag[5]) vh_free_tags(c);
   init_cell_edges(c);
   set_grid_type(c);
   return 0;
@@ -293,6 +298,7 @@ typedef struct {
   vh_ctx *c;
   const vh_medium *m;
   int flim[6][6];
+  uint8_t tag;        /* the painted triple's tag; unused without tags */
 } paint_job;
 
 /* Planes lo..hi-1 of every component's limits. */
@@ -304,6 +310,7 @@ static void paint_range(void *ctx, int lo, int hi)
   for (int f = EX; f <= HZ; f++) {
     double *a = f <= EZ ? c->coef[f] : NULL;
     double *b = f <= EZ ? c->coef[3 + f] : c->coef[6 + f - HX];
+    uint8_t *t = c->ctag[f];
     const int ia = p->flim[f][XLO] > lo ? p->flim[f][XLO] : lo;
     const int ib = p->flim[f][XHI] < hi - 1 ? p->flim[f][XHI] : hi - 1;
     for (int i = ia; i <= ib; i++)
@@ -312,6 +319,7 @@ static void paint_range(void *ctx, int lo, int hi)
           int64_t q = vh_idx(c, i, j, k);
           if (a) { a[q] = m->alpha; b[q] = m->beta; }
           else b[q] = m->gamma;
+          if (t) t[q] = p->tag;
         }
   }
 }
@@ -326,6 +334,52 @@ size_t vh_volume_bytes(size_t n)
  * zeroed on first touch (the painting threads touch them in parallel), so
  * nothing writes the volume twice; advised for huge pages.  Freed by
  * vh_free_volume. */
+static size_t tag_bytes(size_t n)
+{
+  const size_t huge = (size_t)1 << 21;
+  return n ? (n + huge - 1) / huge * huge : huge;
+}
+
+/* A zeroed volume of n bytes, allocated like the double volumes. */
+static uint8_t *alloc_bytes(size_t n)
+{
+  const size_t bytes = tag_bytes(n);
+  void *p = mmap(NULL, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+  if (p == MAP_FAILED) return NULL;
+#ifdef MADV_HUGEPAGE
+  madvise(p, bytes, MADV_HUGEPAGE);
+#endif
+  return p;
+}
+
+void vh_free_tags(vh_ctx *c)
+{
+  const size_t n = (size_t)c->n[0] * c->n[1] * c->n[2];
+  for (int f = 0; f < 6; f++) {
+    if (c->ctag[f]) munmap(c->ctag[f], tag_bytes(n));
+    c->ctag[f] = NULL;
+  }
+  c->num_ctags = 0;
+}
+
+/* The tag of a medium's current (alpha, beta, gamma): the triple's place in
+ * the painted list, plus one.  A medium's coefficients may change between
+ * paintings (a lumped source's), so the tag names the values painted, not
+ * the medium.  A 256th distinct triple drops the tags. */
+static uint8_t medium_tag(vh_ctx *c, const vh_medium *m)
+{
+  if (!c->ctag[0]) return 0;
+  const double v[3] = { m->alpha, m->beta, m->gamma };
+  for (int t = 0; t < c->num_ctags; t++)
+    if (memcmp(c->ctag_coef[t], v, sizeof v) == 0) return (uint8_t)(t + 1);
+  if (c->num_ctags == 255) {
+    vh_free_tags(c);
+    return 0;
+  }
+  memcpy(c->ctag_coef[c->num_ctags], v, sizeof v);
+  return (uint8_t)++c->num_ctags;
+}
+
 static double *alloc_volume(size_t n)
 {
   const size_t bytes = vh_volume_bytes(n);
@@ -350,8 +404,9 @@ void vh_set_medium_on_grid(vh_ctx *c, const int gbbox[6], int medium, unsigned c
   vh_mask_to_bool(incl, mask);
   if (vh_bbox_type(gbbox) == BB_POINT) return;
   vh_set_field_limits(gbbox, flim, incl);
-  paint_job job = { c, &c->media[medium], { 0 } };
+  paint_job job = { c, &c->media[medium], { 0 }, 0 };
   memcpy(job.flim, flim, sizeof flim);
+  job.tag = medium_tag(c, job.m);
   int64_t work = 0;
   for (int f = EX; f <= HZ; f++)
     work += (int64_t)(flim[f][XHI] - flim[f][XLO] + 1) * (flim[f][YHI] - flim[f][YLO] + 1) *
@@ -600,6 +655,7 @@ static void pml_copy_range(void *ctx, int lo, int hi)
           } else {
             c->coef[6 + f - HX][qd] = c->coef[6 + f - HX][qs];
           }
+          if (c->ctag[f]) c->ctag[f][qd] = c->ctag[f][qs];
         }
   }
 }

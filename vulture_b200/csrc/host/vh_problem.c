@@ -136,6 +136,17 @@ int vhost_load(const char *mesh_path, const char *log_path, int verbose, vhost *
 
 /* ---- problem assembly ---- */
 
+/* The assembled problem's medium tags: the painted ones, unless the host
+ * asked for none (vhost_use_tags). */
+static void set_problem_tags(vh_ctx *c)
+{
+  vgpu_problem *p = &c->prob;
+  const int on = c->ctag[0] && c->num_ctags > 0 && !c->tags_off;
+  for (int f = 0; f < 6; f++) p->coef_tag[f] = on ? c->ctag[f] : NULL;
+  p->num_tags = on ? c->num_ctags : 0;
+  p->tag_coef = on ? &c->ctag_coef[0][0] : NULL;
+}
+
 int vh_build_problem(vh_ctx *c, int precision)
 {
   vgpu_problem *p = &c->prob;
@@ -153,6 +164,7 @@ int vh_build_problem(vh_ctx *c, int precision)
     p->idh[a] = c->idh[a];
   }
   for (int q = 0; q < 9; q++) p->coef[q] = c->coef[q];
+  set_problem_tags(c);
   for (int f = 0; f < 6; f++) {
     int t = vh_outer_type(c, f);
     p->ghost[f] = t == BT_PEC ? VGPU_GHOST_PEC : t == BT_PMC ? VGPU_GHOST_PMC
@@ -344,6 +356,34 @@ int vhost_problem(vhost *h, int32_t precision, const vgpu_problem **out)
   return 0;
 }
 
+int vhost_use_tags(vhost *h, int32_t use)
+{
+  if (!h) { vh_set_tls_error("null argument"); return VGPU_EINVAL; }
+  h->tags_off = !use;
+  if (h->prob_ready) set_problem_tags(h);
+  return 0;
+}
+
+int64_t vhost_check_tags(const vhost *h)
+{
+  if (!h || !h->ctag[0] || h->num_ctags == 0) return -1;
+  const int64_t vol = (int64_t)h->n[0] * h->n[1] * h->n[2];
+  const double zero = 0.0;
+  int64_t bad = 0;
+  for (int f = EX; f <= HZ; f++) {
+    const double *a = f <= EZ ? h->coef[f] : NULL;
+    const double *b = f <= EZ ? h->coef[3 + f] : h->coef[6 + f - HX];
+    const uint8_t *t = h->ctag[f];
+    for (int64_t q = 0; q < vol; q++) {
+      if (t[q] > h->num_ctags) { bad++; continue; }
+      const double *v = t[q] ? h->ctag_coef[t[q] - 1] : NULL;
+      const double *ea = v ? &v[0] : &zero, *eb = v ? &v[f <= EZ ? 1 : 2] : &zero;
+      if ((a && memcmp(&a[q], ea, sizeof(double)) != 0) || memcmp(&b[q], eb, sizeof(double)) != 0) bad++;
+    }
+  }
+  return bad;
+}
+
 uint64_t vhost_num_steps(const vhost *h) { return h->num_steps; }
 uint64_t vhost_num_output_steps(const vhost *h)
 {
@@ -383,6 +423,7 @@ void vhost_free(vhost *c)
     free(c->pos_node[a]); free(c->pos_half[a]);
   }
   for (int q = 0; q < 9; q++) vh_free_volume(c->coef[q], (size_t)c->n[0] * c->n[1] * c->n[2]);
+  vh_free_tags(c);
   for (int m = 0; m < c->num_media; m++) {
     free(c->media[m].res); free(c->media[m].pole); free(c->media[m].dalpha); free(c->media[m].dbeta);
   }

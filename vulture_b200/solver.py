@@ -87,6 +87,16 @@ class Mesh:
         """Outer-box cells, the reference's spi/cell denominator."""
         return int(N.lib().vhost_num_cells(self._h))
 
+    def use_tags(self, use: bool = True):
+        """Hand the engine the set-up's medium tags (the default), or leave
+        them out so that it scans the coefficient volumes instead."""
+        N.check_host(N.lib().vhost_use_tags(self._h, int(use)))
+
+    def check_tags(self) -> int:
+        """(cell, component) pairs whose medium tag disagrees with the
+        coefficient volumes; -1 when the set-up kept no tags."""
+        return int(N.lib().vhost_check_tags(self._h))
+
     def observer_name(self, fd: bool, slot: int) -> str:
         return N.lib().vhost_observer_name(self._h, int(fd), slot).decode()
 
