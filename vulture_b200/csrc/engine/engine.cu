@@ -1290,8 +1290,9 @@ struct Engine : EngineBase {
     struct Part {
       int q;                                 // item
       int64_t lo, hi;                        // range of the item's points
-      std::vector<TfsfEntry<T>> single, multi;
-      std::vector<int> spos, mpos, mstart;   // mstart: run starts within multi
+      std::vector<int64_t> sx, mx;           // field indices of single- and multi-entry points
+      std::vector<uint8_t> sq, mq;           // their items
+      std::vector<int> mstart;               // run starts within the multi entries
     };
     std::vector<Part> parts;
     {
@@ -1307,18 +1308,11 @@ struct Engine : EngineBase {
         }
     }
     const int nparts = (int)parts.size();
-    auto make = [&](int q, int i, int j, int k, std::vector<TfsfEntry<T>> &ent, std::vector<int> &pos) {
-      const TfsfItem &it = tv.it[q];
-      // Line length and coefficients are filled in on the device
-      // (k_tfsf_prepare), from the arrays the sweeps read.
-      TfsfEntry<T> d;
-      memset(&d, 0, sizeof d);
-      d.x = (int64_t)i * g.s0 + (int64_t)j * g.s1 + k;
-      d.meta = q;
-      ent.push_back(d);
-      int sp[3] = { i, j, k };
-      sp[it.axis] += it.shift;
-      pos.insert(pos.end(), sp, sp + 3);
+    // An entry is sent as its field index and item; the device fills in the
+    // rest (k_tfsf_prepare), from the arrays the sweeps read.
+    auto make = [&](int q, int i, int j, int k, std::vector<int64_t> &xs, std::vector<uint8_t> &qs) {
+      xs.push_back((int64_t)i * g.s0 + (int64_t)j * g.s1 + k);
+      qs.push_back((uint8_t)q);
     };
     auto enumerate = [&](int w) {
       Part &pt = parts[w];
@@ -1328,8 +1322,8 @@ struct Engine : EngineBase {
       int others[12], no = 0;
       for (int e = 0; e < tv.n; e++)
         if (e != q && tv.it[e].c == it.c && boxes_meet(tv.it[e].b, it.b)) others[no++] = e;
-      pt.single.reserve(pt.hi - pt.lo);
-      pt.spos.reserve(3 * (pt.hi - pt.lo));
+      pt.sx.reserve(pt.hi - pt.lo);
+      pt.sq.reserve(pt.hi - pt.lo);
       const int64_t njk = (int64_t)it.b.nj() * it.b.nk();
       int i = it.b.i0 + (int)(pt.lo / njk), j = it.b.j0 + (int)(pt.lo % njk / it.b.nk()),
           k = it.b.k0 + (int)(pt.lo % it.b.nk());
@@ -1349,13 +1343,13 @@ struct Engine : EngineBase {
         }
         if (!owned) continue;
         if (!followers) {
-          make(q, i, j, k, pt.single, pt.spos);
+          make(q, i, j, k, pt.sx, pt.sq);
           continue;
         }
-        pt.mstart.push_back((int)pt.multi.size());
-        make(q, i, j, k, pt.multi, pt.mpos);
+        pt.mstart.push_back((int)pt.mx.size());
+        make(q, i, j, k, pt.mx, pt.mq);
         for (int o = 0; o < no; o++)
-          if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.multi, pt.mpos);
+          if (others[o] > q && tv.it[others[o]].b.contains(i, j, k)) make(others[o], i, j, k, pt.mx, pt.mq);
       }
     };
     mark(efield ? "tfsf-e-start" : "tfsf-h-start");
@@ -1364,37 +1358,38 @@ struct Engine : EngineBase {
     // Points of one entry first, then the multi-entry points' runs.
     size_t ns = 0, nm = 0;
     for (const Part &pt : parts) {
-      ns += pt.single.size();
-      nm += pt.multi.size();
+      ns += pt.sx.size();
+      nm += pt.mx.size();
     }
     const size_t ne = ns + nm;
     // Each part's runs go to their final offsets, one host thread per part.
     std::vector<size_t> soff(nparts + 1, 0), moff(nparts + 1, ns);
     for (int q = 0; q < nparts; q++) {
-      soff[q + 1] = soff[q] + parts[q].single.size();
-      moff[q + 1] = moff[q] + parts[q].multi.size();
+      soff[q + 1] = soff[q] + parts[q].sx.size();
+      moff[q + 1] = moff[q] + parts[q].mx.size();
     }
     // The merged lists are written where they are sent from: the
     // creation's pinned arena when it has room.
-    std::vector<TfsfEntry<T>> ent_v;
-    std::vector<int> pos_v, mstart;
-    TfsfEntry<T> *ent = (TfsfEntry<T> *)arena_slice(sizeof(TfsfEntry<T>) * ne);
-    int *pos = (int *)arena_slice(sizeof(int) * 3 * ne);
-    if (!ent) {
-      ent_v.resize(ne);
-      ent = ent_v.data();
+    std::vector<int64_t> xs_v;
+    std::vector<uint8_t> qs_v;
+    std::vector<int> mstart;
+    int64_t *xs = (int64_t *)arena_slice(sizeof(int64_t) * ne);
+    uint8_t *qs = (uint8_t *)arena_slice(ne);
+    if (!xs) {
+      xs_v.resize(ne);
+      xs = xs_v.data();
     }
-    if (!pos) {
-      pos_v.resize(3 * ne);
-      pos = pos_v.data();
+    if (!qs) {
+      qs_v.resize(ne);
+      qs = qs_v.data();
     }
     {
       auto place = [&](int q) {
         const Part &pt = parts[q];
-        std::copy(pt.single.begin(), pt.single.end(), ent + soff[q]);
-        std::copy(pt.spos.begin(), pt.spos.end(), pos + 3 * soff[q]);
-        std::copy(pt.multi.begin(), pt.multi.end(), ent + moff[q]);
-        std::copy(pt.mpos.begin(), pt.mpos.end(), pos + 3 * moff[q]);
+        std::copy(pt.sx.begin(), pt.sx.end(), xs + soff[q]);
+        std::copy(pt.sq.begin(), pt.sq.end(), qs + soff[q]);
+        std::copy(pt.mx.begin(), pt.mx.end(), xs + moff[q]);
+        std::copy(pt.mq.begin(), pt.mq.end(), qs + moff[q]);
       };
       HostPool::get().run(nparts, place);
     }
@@ -1407,11 +1402,14 @@ struct Engine : EngineBase {
     tl.nmulti = (int)mstart.size() - 1;
     if (!ne) return 0;
     TfsfEntry<T> *de;
-    int *dpos, *dm;
-    if (upload(&de, ent, ne) || upload(&dpos, pos, 3 * ne) || upload(&dm, mstart.data(), mstart.size()))
+    int64_t *dx;
+    uint8_t *dq;
+    int *dm;
+    if (mem.alloc(&de, ne) || upload(&dx, xs, ne) || upload(&dq, qs, ne) || upload(&dm, mstart.data(), mstart.size()))
       return VGPU_ENOMEM;
     tl.ent = de;
-    tl.pos = dpos;
+    tl.seed_x = dx;
+    tl.seed_q = dq;
     tl.mstart = dm;
     mark("upload");
     k_tfsf_prepare<T><<<blocks_for(ne, 128), 128, 0, ss>>>(g, L.pv, tv, tl, efield ? 1 : 0);

@@ -722,7 +722,8 @@ struct alignas(16) TfsfEntry {
 template <typename T>
 struct TfsfList {
   TfsfEntry<T> *ent;
-  const int *pos;          // incident-field position, 3 ints per entry (set-up only)
+  const int64_t *seed_x;   // set-up only: each entry's field index ...
+  const uint8_t *seed_q;   // ... and item, from which k_tfsf_prepare fills it
   const int *mstart;       // multi-entry points: entry starts, nmulti + 1 values
   int64_t nentries;
   int nsingle, nmulti;
@@ -734,13 +735,21 @@ __global__ void k_tfsf_prepare(Grid<T> g, PwView<T> pw, TfsfView tv, TfsfList<T>
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= tl.nentries) return;
   TfsfEntry<T> &en = tl.ent[e];
+  en.x = tl.seed_x[e];
+  en.meta = tl.seed_q[e];
   const TfsfItem &item = tv.it[en.q()];
   const int c = item.inc;
-  const int i = tl.pos[3 * e], j = tl.pos[3 * e + 1], k = tl.pos[3 * e + 2];
+  // The corrected point (i, j, k) from its field index, and the incident
+  // field's position: the point shifted along the item's axis.
+  const int pi = (int)(en.x / g.s0);
+  const int pj = (int)((en.x - (int64_t)pi * g.s0) / g.s1);
+  const int pk = (int)(en.x - (int64_t)pi * g.s0 - (int64_t)pj * g.s1);
+  const int i = pi + (item.axis == 0 ? item.shift : 0), j = pj + (item.axis == 1 ? item.shift : 0),
+            k = pk + (item.axis == 2 ? item.shift : 0);
   // The corrected point's line length and coefficients, as the sweeps read
-  // them (pos holds the incident-field position, shifted along the axis).
+  // them.
   {
-    const int gi = (item.axis == 0 ? i : item.axis == 1 ? j : k) - item.shift;
+    const int gi = item.axis == 0 ? pi : item.axis == 1 ? pj : pk;
     en.idv = efield ? g.idh[item.axis][gi] : g.ide[item.axis][gi];
     en.ca = efield ? g.coef(item.c, en.x) : (T)0;
     en.cb = efield ? g.coef(3 + item.c, en.x) : g.coef(6 + item.c - HX, en.x);
