@@ -318,6 +318,12 @@ struct SweepLayout {
   static constexpr int NCOEF = ESWEEP ? 6 : 3;
   static constexpr int NAUX = PML ? (ESWEEP ? 6 : 3) : 0;
   static constexpr int S = (sizeof(T) == 8 && PML) ? 3 : 4;   // ring depth
+  // The tile header has two buffers: tile m + 2's stage 0 rewrites tile m's,
+  // and the producer may issue it once stage g - S is released, g being its
+  // place in the ring.  A tile takes at least two stages (stage 0 and one
+  // plane), so g - S reaches tile m's stage 0 -- whose release ends every
+  // read of tile m's header -- only while S <= 4.
+  static_assert(S <= 4, "two header buffers hold only for rings of at most four stages");
   static constexpr int MIN_BLOCKS = sizeof(T) == 4 ? (PML ? 3 : 4) : 2;
   static constexpr uint32_t OWN_B = (uint32_t)(kSweepKW * JH * sizeof(T));
   static constexpr uint32_t OTH_B = (uint32_t)(W * (JH + 1) * sizeof(T));
