@@ -35,6 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 B_ALG = {"fp32": 4, "fp64": 8}        # bytes per word
 WORDS_E, WORDS_H = 15, 12             # algorithmic words per cell of the E and H sweeps
+NOMINAL_HBM_GBS = 8000.0              # the B200's nominal HBM3e bandwidth, for the "% of 8 TB/s" figure
 # The UPML sweeps also read and write their auxiliaries: PP and P per E
 # component (4 words), B per H component (2 words).  These are overhead on
 # the algorithmic basis (not credited in `roofline.achieved`); they appear
@@ -513,7 +514,10 @@ def run_gpu_arm(args):
             "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec],
                               "achieved_gbs": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9,
                               "frac": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9 / peak,
-                              "what": "whole step: cell-updates/s x 27 algorithmic words per cell, of measured"},
+                              "pct_of_8tbs": 100 * value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec]
+                              / 1e9 / NOMINAL_HBM_GBS,
+                              "what": "whole step: cell-updates/s x 27 algorithmic words per cell, of measured; "
+                                      "pct_of_8tbs of the nominal 8 TB/s"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": tr, "kernels": kern,
@@ -623,7 +627,9 @@ def enclosure_workload(args, dist=None, cpu=False):
                                "TFSF, 128x128 + 8 FD points x 500 frequencies, 20000 steps",
                    "n_out_cells": n_out, "precision": prec, "dft": "fp64"},
         "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec],
-                          "frac": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9 / peak},
+                          "frac": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9 / peak,
+                          "pct_of_8tbs": 100 * value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9
+                          / NOMINAL_HBM_GBS},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": kern[dom]["gbs"] / peak, "kernels": kern},
         "kernel_split": split,
@@ -763,6 +769,8 @@ def batch_workload(args, dist=None):
         "mcell_updates_per_s_e2e": cell_updates / wall32 / 1e6,
         "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG["fp32"],
                           "frac": step_mcell * 1e6 * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9 / peak / world,
+                          "pct_of_8tbs": 100 * step_mcell * 1e6 * (WORDS_E + WORDS_H) * B_ALG["fp32"] / 1e9
+                          / NOMINAL_HBM_GBS / world,
                           "peak": peak, "peak_kind": peak_kind,
                           "what": "stepping: cell-updates/s x 27 algorithmic words per cell, of measured"},
         "sweep_bytes_gbs_with_upml_aux": nbytes / step_s / 1e9 / world,
