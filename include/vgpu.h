@@ -238,7 +238,8 @@ typedef struct {
    * (coef[3 + f]) for an H one.  When set they must describe coef[] exactly;
    * vgpu_create then finds the distinct coefficient tuples from three bytes
    * per cell for E and three for H instead of the nine double volumes.  All
-   * NULL (or num_tags 0): it scans coef[]. */
+   * NULL (or num_tags 0): it scans coef[].  A tag above num_tags makes
+   * vgpu_create return VGPU_EINVAL. */
   const uint8_t *coef_tag[6];
   int32_t num_tags;           /* at most 255 */
   const double *tag_coef;     /* [num_tags][3]: alpha, beta, gamma */

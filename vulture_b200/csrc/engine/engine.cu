@@ -1443,6 +1443,7 @@ struct Engine : EngineBase {
     struct Part {
       std::vector<Key> keys;   // local tuples in first-seen order
       bool overflow = false;
+      int bad_tag = 0;         // a tag past the problem's table, if met
     };
     std::vector<Part> parts(nthr);
     // With medium tags a cell's tuple follows from its components' tag bytes
@@ -1493,6 +1494,10 @@ struct Engine : EngineBase {
             Key key{};
             for (int c = 0; c < count; c++) {
               const uint8_t tc = t[vol_tag[c]];
+              if (tc > p.num_tags) {
+                pt.bad_tag = tc;
+                return;
+              }
               key.v[c] = tc ? (T)p.tag_coef[(tc - 1) * 3 + vol_slot[c]] : (T)0.0;
             }
             int q = -1;
@@ -1578,6 +1583,9 @@ struct Engine : EngineBase {
       HostPool::get().run(nthr, work_tags);
     else
       HostPool::get().run(nthr, work);
+    for (const Part &pt : parts)
+      if (pt.bad_tag)
+        return set_err(VGPU_EINVAL, "medium tag %d is past the problem's %d tags", pt.bad_tag, (int)p.num_tags);
     // Merge: global numbers in plane order, then renumber each part's planes.
     std::map<Key, int> global;
     std::vector<T> table;
