@@ -194,6 +194,17 @@ def traffic_record(kernel: str, precision: str):
     return d.get(f"{kernel}:{precision}")
 
 
+def scaled_traffic(kernel: str, precision: str, cells: float):
+    """DRAM bytes per launch of a kernel whose ncu capture ran on a smaller
+    case of the same workload ({"bytes": B, "cells": C} in traffic.json):
+    B scaled by the cells this launch updates, since the traffic grows in
+    proportion.  A plain number is already per launch at full size."""
+    rec = traffic_record(kernel, precision)
+    if isinstance(rec, dict):
+        return rec["bytes"] * cells / rec["cells"]
+    return rec
+
+
 def time_reference(binary: str, mesh_dir: Path, nt_lo: int, nt_hi: int, threads: int, plane=None):
     """Per-step throughput of a reference build: two runs of the same mesh
     with nt_lo and nt_hi steps; the difference removes set-up and output.
@@ -578,7 +589,8 @@ def enclosure_workload(args, dist=None, cpu=False):
 
     rank, world, local = rank_info()
     work = Path(tempfile.mkdtemp(prefix=f"vb_encl_{rank}_"))
-    text = meshgen.shielded_enclosure(seed=3, nt=20000, dims=(400, 300, 250), plane=128, nfreq=500)
+    dims = tuple(getattr(args, "enclosure_dims", None) or (400, 300, 250))
+    text = meshgen.shielded_enclosure(seed=3, nt=20000, dims=dims, plane=128, nfreq=500)
     path = Path(meshgen.write(text, work / "enclosure.mesh"))
     m = vb.Mesh(path)
     n_out = m.num_cells
@@ -623,15 +635,16 @@ def enclosure_workload(args, dist=None, cpu=False):
         "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "dtype": prec,
         "untimed_steps_before": PREHEAT_STEPS + args.warmup,
-        "config": {"workload": "shielded enclosure 400x300x250 graded, Mur, SIBC box with aperture, 4 PEC wires, "
-                               "TFSF, 128x128 + 8 FD points x 500 frequencies, 20000 steps",
+        "config": {"workload": "shielded enclosure {}x{}x{} graded, Mur, SIBC box with aperture, 4 PEC wires, "
+                               "TFSF, 128x128 + 8 FD points x 500 frequencies, 20000 steps".format(*dims),
                    "n_out_cells": n_out, "precision": prec, "dft": "fp64"},
         "step_roofline": {"bytes_per_cell": (WORDS_E + WORDS_H) * B_ALG[prec],
                           "frac": value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9 / peak,
                           "pct_of_8tbs": 100 * value / world * 1e6 * (WORDS_E + WORDS_H) * B_ALG[prec] / 1e9
                           / NOMINAL_HBM_GBS},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": kern[dom]["gbs"] / peak, "kernels": kern},
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": kern[dom]["gbs"] / peak,
+                     "traffic": scaled_traffic(dom, prec, kern[dom]["cells"]), "kernels": kern},
         "kernel_split": split,
         "e2e_full_run": full,
         "clocks": clk.summary()}
@@ -642,7 +655,7 @@ def enclosure_workload(args, dist=None, cpu=False):
             walls = []
             for nt in (2, 6):
                 d = Path(tempfile.mkdtemp(prefix="vb_cpue_", dir=work))
-                meshgen.write(meshgen.shielded_enclosure(seed=3, nt=nt, dims=(400, 300, 250), plane=128, nfreq=500),
+                meshgen.write(meshgen.shielded_enclosure(seed=3, nt=nt, dims=dims, plane=128, nfreq=500),
                               d / "enclosure.mesh")
                 t0 = time.perf_counter()
                 r = subprocess.run([str(binary), "-n", str(threads), "enclosure.mesh"], cwd=d, capture_output=True,
@@ -904,6 +917,9 @@ def main():
                     help="without the whole-run e2e legs (and the graded workload's FP32-error leg)")
     ap.add_argument("--no-batch", action="store_true", help="graded workload without the batch sub-object")
     ap.add_argument("--no-serve", action="store_true", help="graded workload without the serve sub-object")
+    ap.add_argument("--enclosure-dims", type=int, nargs=3, default=[400, 300, 250],
+                    help="cells per axis of the enclosure workload (its stated size by default; smaller for an ncu "
+                         "capture)")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, nargs=2, default=[2000, 8000])
     ap.add_argument("--batch-fp64-sample", type=int, default=32)
