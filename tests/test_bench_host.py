@@ -56,3 +56,16 @@ def test_error_report_without_a_matching_reference_run(tmp_path, monkeypatch):
     re = np.ones((1, 6, 3))
     rep = bench.error_report(td, re, re * 0, td, re, re * 0, 4, ["p0"])
     assert "vs_reference_fp32" not in rep and rep["fd_db_max"] == 0.0
+
+
+def test_traffic_records_scale_by_cells(tmp_path, monkeypatch):
+    # A record captured on a smaller case scales with the cells a launch
+    # updates; a plain number is already per launch at full size.
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    (prof / "traffic.json").write_text(json.dumps({"k<E,bulk>:fp32": {"bytes": 200, "cells": 10},
+                                                   "k<E,UPML>:fp32": 1234}))
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    assert bench.scaled_traffic("k<E,bulk>", "fp32", 25.0) == 500.0
+    assert bench.scaled_traffic("k<E,UPML>", "fp32", 99.0) == 1234
+    assert bench.scaled_traffic("k<H,bulk>", "fp32", 1.0) is None
