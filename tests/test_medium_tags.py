@@ -53,3 +53,16 @@ def test_too_many_triples_keep_no_tags():
     m.use_tags(True)      # nothing to put back: still none
     assert m.check_tags() == -1
     m.close()
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_tags_describe_volumes_of_random_meshes(seed):
+    # Batch and serving meshes from other seeds: random media, slabs, sizes,
+    # UPML or Mur, Debye blocks and plane waves.
+    rng = random.Random(100 + seed)
+    for q in range(4):
+        text = (meshgen.batch_mesh(rng, q, nmin=16, nmax=40, ntmin=5, ntmax=10) if q % 2 == 0 else
+                meshgen.serving_request(rng, q, nmin=20, nmax=44, ntmin=5, ntmax=10))
+        m = vb.Mesh(stage_text(text, f"r{seed}_{q}.mesh"))
+        assert m.check_tags() == 0
+        m.close()
