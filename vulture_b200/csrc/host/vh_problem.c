@@ -5,6 +5,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "vh.h"
 
@@ -85,8 +86,28 @@ static void report_mesh(vh_ctx *c)
   vh_log(c, 0, "  Number of observers: %lu\n", (unsigned long)c->num_obs);
 }
 
+/* With VHOST_TRACE set, vhost_load prints the time of each set-up phase to
+ * stderr. */
+typedef struct {
+  int on, len;
+  struct timespec t;
+  char buf[512];
+} load_clock;
+
+static void load_mark(load_clock *lc, const char *name)
+{
+  if (!lc->on) return;
+  struct timespec now;
+  clock_gettime(CLOCK_MONOTONIC, &now);
+  const double ms = (now.tv_sec - lc->t.tv_sec) * 1e3 + (now.tv_nsec - lc->t.tv_nsec) * 1e-6;
+  lc->t = now;
+  if (lc->len < (int)sizeof lc->buf - 40) lc->len += snprintf(lc->buf + lc->len, sizeof lc->buf - lc->len, " %s %.2f", name, ms);
+}
+
 int vhost_load(const char *mesh_path, const char *log_path, int verbose, vhost **out)
 {
+  load_clock lc = { getenv("VHOST_TRACE") != NULL, 0, { 0, 0 }, { 0 } };
+  if (lc.on) clock_gettime(CLOCK_MONOTONIC, &lc.t);
   *out = NULL;
   vh_ctx *c = calloc(1, sizeof(vh_ctx));
   if (!c) { vh_set_tls_error("out of memory"); return VGPU_ENOMEM; }
@@ -109,27 +130,35 @@ int vhost_load(const char *mesh_path, const char *log_path, int verbose, vhost *
     if (c->courant < 0.0) c->courant = sqrt(3.0) / 2.0;
     report_mesh(c);
   }
+  load_mark(&lc, "read");
   if (!rc) rc = vh_init_grid(c);
   if (!rc) {
     for (int b = 0; b < c->num_bnds && !rc; b++)
       if (c->bnds[b].type == BT_SIBC) rc = vh_init_sibc_boundary(c, &c->bnds[b]);
   }
+  load_mark(&lc, "grid");
   if (!rc) rc = vh_init_media(c);
   if (!rc) vh_init_media_arrays(c);
+  load_mark(&lc, "media");
   if (!rc) rc = vh_init_blocks(c);
   if (!rc) rc = vh_init_lines(c);
   if (!rc) rc = vh_init_internal_surfaces(c);
   if (!rc) rc = vh_init_external_surfaces(c);
+  load_mark(&lc, "blocks-lines-surfaces");
   if (!rc) rc = vh_init_waveforms(c);
   if (!rc) rc = vh_init_sources(c);
   if (!rc) rc = vh_init_planewaves(c);
+  load_mark(&lc, "sources-planewaves");
   if (!rc) rc = vh_init_observers(c);
+  load_mark(&lc, "observers");
   if (rc) {
     vh_set_tls_error(c->err);
     vhost_free(c);
     return VGPU_EINVAL;
   }
   report_grid(c);
+  load_mark(&lc, "report");
+  if (lc.on) fprintf(stderr, "vhost load (ms):%s\n", lc.buf);
   *out = c;
   return 0;
 }
